@@ -1,0 +1,187 @@
+/*
+ * ltlgpu — C ABI of the B200 characteristic-set (CS) enumerator.
+ *
+ * This is the drop-in boundary for the reference's enumeration entry
+ *     std::string LTLI(const unsigned short *costFun, unsigned short maxCost,
+ *                      unsigned RlxUnqChkTyp, unsigned NegType, std::set<char> alphabet,
+ *                      int &LTLcost, std::uint64_t &allLTLs,
+ *                      vector<vector<string>> pos, vector<vector<string>> neg)
+ * (MojtabaValizadeh/ltl-learning-on-gpus, code/ltli6463.cu:1043-1052), restated with plain
+ * pointers and sizes.  The ltli6463-compatible executable (csrc/cli_ltli6463.cpp) and the
+ * Python bindings call only what is declared here.
+ *
+ * Conventions
+ *   - Traces: positives first, then negatives.  Each time step is a uint32 mask with
+ *     bit (letter - 'a') set when that letter holds; offsets[t] .. offsets[t + 1] are the
+ *     steps of trace t.  This is the reference's token strings (ltli6463.cu:1526-1565)
+ *     packed into bits.
+ *   - The alphabet is the sorted letter string (the reference's std::set<char> order); the
+ *     letter at index j is CS row j.
+ *   - Operator codes are the reference's region index i % 7 (ltli6463.cu:892-926):
+ *     0 ~, 1 &, 2 |, 3 X, 4 F, 5 G, 6 U; 7 marks a letter row.
+ *   - Status codes replace the reference's sentinel strings ("not_found",
+ *     "see_the_error", "Size of the output is too big"); the formula string keeps the
+ *     sentinel text so string-level callers see what the reference printed.
+ *   - The caller owns every input buffer.  The library allocates the result's arrays and
+ *     frees them in ltlg_result_free.  An engine is not thread-safe: one host thread per
+ *     engine (each engine owns its own CUDA stream and device buffers).
+ */
+#ifndef LTLGPU_H
+#define LTLGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LTLG_API __attribute__((visibility("default")))
+#define LTLG_ABI_VERSION 1
+
+typedef struct ltlg_traces {
+    int32_t num_pos;
+    int32_t num_neg;
+    const char *alphabet;      /* sorted letters, NUL terminated */
+    const uint32_t *steps;     /* per time step, bit (letter - 'a') */
+    const int32_t *offsets;    /* num_pos + num_neg + 1 entries, offsets[0] == 0 */
+} ltlg_traces;
+
+enum ltlg_key_mode {
+    LTLG_KEY_EXACT = 0,        /* uniqueness on the full CS (verified word by word) */
+    LTLG_KEY_REF = 1,          /* the reference's relaxed keys, type = rlx_unq_chk_type (ltli6463.cu:57-141) */
+    LTLG_KEY_HASH64 = 2        /* relaxed: a 64-bit fingerprint of the full CS, not verified */
+};
+
+enum ltlg_schedule {
+    LTLG_SCHEDULE_FUSED = 0,   /* one persistent launch per level drains every block of the level */
+    LTLG_SCHEDULE_PER_BLOCK = 1 /* one launch per (operator, split) block, in order; per-block stats */
+};
+
+enum ltlg_order {
+    LTLG_ORDER_PLAIN = 0,      /* the reference's operator / split order (ltli6463.cu:1209-1440) */
+    LTLG_ORDER_LEARNED = 1     /* blocks of a level sorted by the loaded scorer, highest first */
+};
+
+enum ltlg_status {
+    LTLG_FOUND = 0,
+    LTLG_NOT_FOUND = 1,
+    LTLG_INPUT_LIMITS = 2,     /* more than 63 steps in a trace (or > 64 traces with limit_traces) */
+    LTLG_TIMEOUT = 3,
+    LTLG_NO_MEMORY = 4,
+    LTLG_BAD_ARGS = 5,
+    LTLG_CUDA_ERROR = 6,
+    LTLG_DEVICE_WAIT = 7,      /* a bounded device-side wait gave up; results are not trusted */
+    LTLG_TABLE_FULL = 8,
+    LTLG_NO_DEVICE = 9
+};
+
+typedef struct ltlg_engine_config {
+    int32_t device;            /* CUDA device ordinal */
+    int32_t slots_log2;        /* hash-set slots = 2^slots_log2 (8-byte slots) */
+    int64_t cache_bytes;       /* language-cache budget in bytes (rows = budget / (8 * pitch)) */
+    int64_t max_rows;          /* upper bound on cache rows (<= 2^30); 0 = budget only */
+    int32_t max_traces;        /* largest n the engine accepts */
+    int32_t block_threads;     /* threads per CTA of the level kernel (multiple of 32) */
+    int32_t left_tile;         /* left rows staged in shared memory per binary work item: 4, 8 or 16 */
+    int32_t right_chunk;       /* right rows per binary work item */
+    int32_t unary_rows;        /* source rows per unary work item */
+    int32_t pad_;
+} ltlg_engine_config;
+
+typedef struct ltlg_options {
+    int32_t cost_fun[8];       /* p ~ & | X F G U, each in 1..SHRT_MAX */
+    int32_t max_cost;
+    int32_t rlx_unq_chk_type;  /* the reference's argument 11 (1, 2, 3), used with LTLG_KEY_REF */
+    int32_t neg_type;          /* 1: negate every formula, 2: negate letters only (ltli6463.cu:1212) */
+    int32_t key_mode;          /* ltlg_key_mode */
+    int32_t schedule;          /* ltlg_schedule */
+    int32_t order;             /* ltlg_order */
+    int32_t stop_at_found;     /* 1: stop at the first accepting candidate; 0: enumerate to max_cost */
+    int32_t limit_traces;      /* 1: apply the reference's 64-trace limit too (ltli6463.cu:1078) */
+    int32_t record_levels;     /* 1: time each level with CUDA events */
+    int32_t pad_;
+    double time_limit_s;       /* > 0: stop between levels once exceeded */
+} ltlg_options;
+
+typedef struct ltlg_level_stat {
+    int32_t cost;
+    int32_t blocks;
+    uint64_t candidates;       /* candidates the device evaluated at this cost */
+    uint64_t uniques;          /* rows stored at this cost */
+    double ms;                 /* device time of the level (record_levels) */
+} ltlg_level_stat;
+
+typedef struct ltlg_block_stat {
+    int32_t cost;
+    int32_t op;                /* operator code */
+    int32_t left_cost;         /* split: cost of the left operand (unary: operand cost) */
+    int32_t right_cost;
+    int64_t stored_before;     /* rows stored when the block started (the reference's StoredLTLs) */
+    uint64_t all_before;       /* candidates counted before the block (the reference's AllLTLs) */
+    int64_t to_check;          /* candidates in the block (the reference's ToBeChecked) */
+} ltlg_block_stat;
+
+typedef struct ltlg_result {
+    int32_t status;            /* ltlg_status */
+    int32_t cost;              /* LTLcost as the reference reports it */
+    uint64_t all_ltls;         /* candidates counted as the reference counts them */
+    uint64_t evaluated;        /* candidates the device actually evaluated */
+    int64_t rows;              /* rows in the language cache (letters included) */
+    char *formula;             /* the reference's string format, or its sentinel text */
+    double seconds;            /* host wall time of the call */
+    double device_ms;          /* device time of the level loop */
+    int32_t num_levels;
+    int32_t num_blocks;
+    ltlg_level_stat *levels;
+    ltlg_block_stat *blocks;   /* filled with LTLG_SCHEDULE_PER_BLOCK */
+    int32_t found_op;          /* root operator of the returned formula (7 for a letter) */
+    uint32_t device_flags;     /* raw device status bits (overflow, waits, table) */
+    int32_t on_the_fly;        /* 1 once the cache overflowed (the reference's onTheFly) */
+    int32_t pad_;
+} ltlg_result;
+
+typedef struct ltlg_engine ltlg_engine;
+
+/* Defaults: device 0, 2^27 slots, 16 GiB cache, n <= 8192, 256 threads, tiles 8/64/64. */
+LTLG_API void ltlg_default_engine_config(ltlg_engine_config *cfg);
+/* The reference's defaults: unit costs, maxCost 500, type 3, NegType 2, exact keys, fused, plain. */
+LTLG_API void ltlg_default_options(ltlg_options *opt);
+
+LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg, ltlg_engine **out);
+LTLG_API void ltlg_engine_destroy(ltlg_engine *eng);
+
+/* Learn one formula.  Replaces LTLI (ltli6463.cu:1043); the engine's buffers are reused. */
+LTLG_API int ltlg_engine_learn(ltlg_engine *eng, const ltlg_traces *traces, const ltlg_options *opt,
+                               ltlg_result *res);
+
+/* One-shot form: creates an engine sized for the input, learns, destroys it. */
+LTLG_API int ltlg_learn(const ltlg_traces *traces, const ltlg_options *opt, ltlg_result *res);
+
+LTLG_API void ltlg_result_free(ltlg_result *res);
+
+/* After a learn: copy cache rows [first, first + count) (n words each, pitch dropped) and
+ * their packed parents (op << 60 | left << 30 | right) to host memory.  Either pointer may
+ * be NULL.  Returns 0 or an ltlg_status. */
+LTLG_API int ltlg_engine_read_rows(ltlg_engine *eng, int64_t first, int64_t count, uint64_t *rows,
+                                   uint64_t *parents);
+/* Row ranges of each cost after a learn: starts[c] for c in 0..max_cost + 1. */
+LTLG_API int ltlg_engine_level_starts(ltlg_engine *eng, int64_t *starts, int32_t count);
+
+/* Device building blocks, for kernel-level parity tests (device buffers are allocated
+ * and freed inside; host arrays in and out). */
+LTLG_API int ltlg_device_apply_op(int32_t op, const uint64_t *a, const uint64_t *b, const uint64_t *lenmask,
+                                  int32_t n, int32_t count, uint64_t *out, uint64_t *out2, uint64_t *fp);
+
+/* Scarlet file reader with the reference's rules (ltli6463.cu:1500-1573).  Allocates the
+ * arrays inside *out; release with ltlg_traces_free. Returns 0 or LTLG_BAD_ARGS. */
+LTLG_API int ltlg_read_scarlet(const char *path, ltlg_traces *out);
+LTLG_API void ltlg_traces_free(ltlg_traces *t);
+
+LTLG_API const char *ltlg_status_string(int status);
+LTLG_API int ltlg_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

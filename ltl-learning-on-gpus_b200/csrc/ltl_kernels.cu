@@ -1,0 +1,819 @@
+// Characteristic-set (CS) enumeration kernels for sm_100a.
+//
+// One persistent launch per cost level drains a device work queue of items cut
+// from the level's (operator, split) blocks.  A binary item stages a tile of
+// left-operand CSs in shared memory with one bulk copy (cp.async.bulk, no
+// multicast) and streams right-operand CSs from HBM with 128-bit loads; every
+// warp evaluates a whole tile of candidates per right row in registers.  The
+// fused epilogue per candidate is: fingerprint (warp reduce-scatter),
+// acceptance (redux.sync over bit 0 of every word), and exact uniqueness in an
+// open-addressing HBM hash set (claim by CAS, write the row, publish; a
+// fingerprint match is verified word by word against the stored row).
+//
+// Semantics follow MojtabaValizadeh/ltl-learning-on-gpus, code/ltli6463.cu:
+//   operators .......... :203-204 (~), :295 (&), :385 (|), :468 (X), :551-556 (F),
+//                        :638-645 (G), :739-771 (U, both orders from one pair)
+//   acceptance ......... :240-243 (positives need bit 0 set, negatives clear)
+//   uniqueness ......... :224-231 (a candidate is stored iff its key is new)
+//   relaxed keys ....... :57-141 (KEY_REF, types 1/2/3 and the exact 126-bit pack)
+//   found .............. :243 (atomicCAS on a found word)
+// Every device wait is bounded; giving up sets a status bit the host reads.
+#include "ltl_kernels.cuh"
+
+namespace ltlg {
+
+namespace {
+
+constexpr u64 WEYL = 0x9E3779B97F4A7C15ull;
+constexpr u64 LENMASK = 0x7FFFFFFFFFFFFFFFull;
+constexpr u64 M63 = 0x7FFFFFFFFFFFFFFFull;
+constexpr u32 FIELD_PENDING = 0xFFFFFFFFu;
+constexpr u32 FIELD_OVERFLOW = 0xFFFFFFFEu;
+constexpr unsigned FULL = 0xFFFFFFFFu;
+constexpr long long WAIT_SPINS = 1ll << 22;    // slot publication wait (with nanosleep): ~1 s
+constexpr long long MBAR_SPINS = 1ll << 24;    // bulk-copy completion wait
+constexpr int UNARY_GROUP = 4;                 // source rows a warp evaluates together
+
+// MurmurHash3's 64-bit finaliser (Appleby, public domain).
+__device__ __forceinline__ u64 fmix64(u64 x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+__device__ __forceinline__ u64 smear(u64 w) {
+    w |= w >> 1;
+    w |= w >> 2;
+    w |= w >> 4;
+    w |= w >> 8;
+    w |= w >> 16;
+    w |= w >> 32;
+    return w;
+}
+
+// x U y: y holds, or x holds and (x U y) holds one step later; log-step doubling.
+__device__ __forceinline__ u64 until_bits(u64 x, u64 y) {
+    y |= x & (y >> 1);
+    x &= x >> 1;
+    y |= x & (y >> 2);
+    x &= x >> 2;
+    y |= x & (y >> 4);
+    x &= x >> 4;
+    y |= x & (y >> 8);
+    x &= x >> 8;
+    y |= x & (y >> 16);
+    x &= x >> 16;
+    y |= x & (y >> 32);
+    return y;
+}
+
+template <int OP>
+__device__ __forceinline__ u64 uop(u64 w, u64 meta) {
+    const u64 m = meta & LENMASK;
+    if (OP == OP_NEG) return ~w & m;
+    if (OP == OP_X) return w >> 1;
+    if (OP == OP_F) return smear(w);
+    return w & ~smear(~w & m);  // OP_G
+}
+
+template <int OP>
+__device__ __forceinline__ u64 bop(u64 a, u64 b) {
+    if (OP == OP_AND) return a & b;
+    if (OP == OP_OR) return a | b;
+    return until_bits(a, b);
+}
+
+// Word i of a CS contributes fmix64(w ^ (i + 1) * WEYL) to the fingerprint sum.
+__device__ __forceinline__ u64 hw(u64 w, u64 key, bool valid) { return valid ? fmix64(w ^ key) : 0ull; }
+// Bit 0 disagrees with the label (positives need 1, negatives 0); padding words are 0 with label 0.
+__device__ __forceinline__ u32 badbit(u64 w0, u64 w1, u64 m0, u64 m1) {
+    return (u32)(((w0 ^ (m0 >> 63)) | (w1 ^ (m1 >> 63))) & 1ull);
+}
+
+__device__ __forceinline__ u64 ld_acquire(const u64 *p) {
+    u64 v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(u64 *p, u64 v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ u64 ld_volatile(const u64 *p) { return *(const volatile u64 *)p; }
+
+// ---------------------------------------------------------------- mbarrier + bulk copy
+__device__ __forceinline__ u32 smem_u32(const void *p) { return (u32)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(u64 *bar, u32 count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(u64 *bar, u32 bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// 1-D bulk copy global -> shared (no multicast); both addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, u32 bytes, u64 *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(u64 *bar, u32 parity) {
+    u32 ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(u64 *bar, u32 parity) {
+    for (long long i = 0; i < MBAR_SPINS; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// ---------------------------------------------------------------- warp reductions
+// Sum v[t] over the warp for NC = 2^K candidates with a reduce-scatter
+// (NC - 1 + 5 - K shuffles instead of 5 NC); lane t (< NC) gets candidate t.
+template <int NC>
+__device__ __forceinline__ u64 reduce_to_lane(u64 (&v)[NC], int lane) {
+    constexpr int K = NC == 1 ? 0 : NC == 2 ? 1 : NC == 4 ? 2 : NC == 8 ? 3 : NC == 16 ? 4 : 5;
+    static_assert((1 << K) == NC, "NC must be a power of two <= 32");
+#pragma unroll
+    for (int s = 0; s < K; ++s) {
+        const int o = 16 >> s;
+        constexpr int dummy = 0;
+        (void)dummy;
+        const bool upper = (lane & o) != 0;
+        const int half = NC >> (s + 1);
+#pragma unroll
+        for (int j = 0; j < NC / 2; ++j) {
+            if (j < half) {
+                const u64 send = upper ? v[j] : v[j + half];
+                const u64 keep = upper ? v[j + half] : v[j];
+                v[j] = keep + __shfl_xor_sync(FULL, send, o);
+            }
+        }
+    }
+    u64 x = v[0];
+#pragma unroll
+    for (int o = 16 >> K; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+    return __shfl_sync(FULL, x, (lane << (5 - K)) & 31);
+}
+
+// ---------------------------------------------------------------- candidate generators
+// word2(t, c) recomputes words 2c, 2c+1 of candidate t.
+template <int OP>
+struct BinGen {
+    const ulonglong2 *left;   // shared-memory tile, row stride nch
+    const ulonglong2 *right;  // global right row
+    int nch;
+    __device__ __forceinline__ ulonglong2 word2(int t, int c) const {
+        const ulonglong2 r = right[c];
+        if (OP == OP_U) {
+            const ulonglong2 l = left[(t >> 1) * nch + c];
+            if (t & 1) return make_ulonglong2(until_bits(r.x, l.x), until_bits(r.y, l.y));
+            return make_ulonglong2(until_bits(l.x, r.x), until_bits(l.y, r.y));
+        }
+        const ulonglong2 l = left[t * nch + c];
+        return make_ulonglong2(bop<OP>(l.x, r.x), bop<OP>(l.y, r.y));
+    }
+};
+
+template <int OP>
+struct UnGen {
+    const u64 *src0;  // first source row of the group; rows are consecutive
+    const ulonglong2 *meta;
+    int pitch;
+    __device__ __forceinline__ ulonglong2 word2(int t, int c) const {
+        const ulonglong2 s = reinterpret_cast<const ulonglong2 *>(src0 + (size_t)t * pitch)[c];
+        const ulonglong2 m = __ldg(meta + c);
+        return make_ulonglong2(uop<OP>(s.x, m.x), uop<OP>(s.y, m.y));
+    }
+};
+
+// A stored row as its own candidate (letters).
+struct RowGen {
+    const ulonglong2 *r;
+    __device__ __forceinline__ ulonglong2 word2(int, int c) const { return r[c]; }
+};
+
+// Relaxed key of candidate t (KEY_REF), warp-cooperative; result valid in every lane.
+template <class Gen>
+__device__ void ref_key(const LevelArgs &A, const Gen &g, int t, int lane, u64 &kh, u64 &kl) {
+    const int nch = A.pitch >> 1;
+    u64 h = 0, l = 0;
+    for (int c = lane; c < nch; c += 32) {
+        const ulonglong2 w2 = g.word2(t, c);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int i = 2 * c + e;
+            if (i >= A.n) break;
+            const u64 w = e ? w2.y : w2.x;
+            if (A.rlx_type == 3) {
+                // splitmix64 finaliser per word, folded by halves (ltli6463.cu:108-119)
+                u64 x = w;
+                x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+                x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+                x = x ^ (x >> 31);
+                if (i < A.n / 2)
+                    h ^= x;
+                else
+                    l ^= x;
+            } else {
+                const u32 km = A.kmeta[i];
+                const u32 start = km & 0xFFFFu, count = (km >> 16) & 0xFFu, step = km >> 24;
+                if (start >= 126 || count == 0) continue;
+                u64 bits;
+                if (step <= 1) {
+                    bits = count >= 64 ? w : (w & ((1ull << count) - 1));
+                } else {
+                    bits = 0;
+                    for (u32 q = 0; q < count; ++q) bits |= ((w >> (q * step)) & 1ull) << q;
+                }
+                const unsigned __int128 v = (unsigned __int128)bits << start;
+                l |= (u64)v & M63;
+                h |= (u64)(v >> 63) & M63;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const u64 ho = __shfl_xor_sync(FULL, h, o), lo = __shfl_xor_sync(FULL, l, o);
+        if (A.rlx_type == 3) {
+            h ^= ho;
+            l ^= lo;
+        } else {
+            h |= ho;
+            l |= lo;
+        }
+    }
+    kh = h;
+    kl = l;
+}
+
+// ---------------------------------------------------------------- uniqueness
+enum { S_DONE = 0, S_PROBE = 1, S_CLAIM = 2, S_WAIT = 3, S_VERIFY = 4 };
+
+__device__ __forceinline__ bool slot_free(u64 v, u32 gen) { return v == 0 || (u32)((v >> 32) & 0xFFu) != gen; }
+
+// Lane t owns candidate t (t < NC).  Claims are written and published before any
+// lane of the warp waits on another warp's publication, so waits cannot cycle.
+template <class Gen>
+__device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u64 parent, u64 kh, u64 kl,
+                        int lane) {
+    int state = active ? S_PROBE : S_DONE;
+    const u64 tagbits = (fp >> 40) << 40;
+    const u64 genbits = (u64)A.gen << 32;
+    u64 idx = fp & A.slot_mask;
+    long long vrow = -1;
+    u64 probes = 0;
+    const int nch = A.pitch >> 1;
+    while (__any_sync(FULL, state != S_DONE)) {
+        if (state == S_PROBE) {
+            for (;;) {
+                u64 *sp = A.slots + idx;
+                u64 v = ld_acquire(sp);
+                if (slot_free(v, A.gen)) {
+                    const u64 old = atomicCAS(sp, v, tagbits | genbits | FIELD_PENDING);
+                    if (old == v) {
+                        state = S_CLAIM;
+                        break;
+                    }
+                    v = old;
+                    if (slot_free(v, A.gen)) continue;
+                }
+                if ((v >> 40) == (tagbits >> 40)) {
+                    const u32 f = (u32)v;
+                    if (f == FIELD_PENDING) {
+                        state = S_WAIT;
+                        break;
+                    }
+                    if (f == FIELD_OVERFLOW) {
+                        state = S_DONE;
+                        break;
+                    }
+                    vrow = (long long)f - 1;
+                    state = S_VERIFY;
+                    break;
+                }
+                idx = (idx + 1) & A.slot_mask;
+                if (++probes > A.slot_mask) {
+                    atomicOr(&A.ctl->status, ST_TABLE);
+                    state = S_DONE;
+                    break;
+                }
+            }
+        }
+        // Claims: reserve rows (one atomic per warp), write the CSs, publish.
+        const u32 cm = __ballot_sync(FULL, state == S_CLAIM);
+        if (cm) {
+            const int leader = __ffs(cm) - 1;
+            u64 base = 0;
+            if (lane == leader) base = atomicAdd(&A.ctl->row_count, (u64)__popc(cm));
+            base = __shfl_sync(FULL, base, leader);
+            u32 rem = cm;
+            while (rem) {
+                const int t = __ffs(rem) - 1;
+                rem &= rem - 1;
+                const u64 row = base + __popc(cm & ((1u << t) - 1));
+                if (row < (u64)A.cap_rows) {
+                    ulonglong2 *dst = reinterpret_cast<ulonglong2 *>(A.cache + row * (u64)A.pitch);
+                    for (int c = lane; c < nch; c += 32) dst[c] = g.word2(t, c);
+                }
+            }
+            u64 myrow = base + __popc(cm & ((1u << lane) - 1));
+            if (state == S_CLAIM && myrow < (u64)A.cap_rows) {
+                A.parents[myrow] = parent;
+                if (A.keys) {
+                    A.keys[2 * myrow] = kh;
+                    A.keys[2 * myrow + 1] = kl;
+                }
+            }
+            __threadfence();
+            __syncwarp();
+            if (state == S_CLAIM) {
+                u32 f = FIELD_OVERFLOW;
+                if (myrow < (u64)A.cap_rows)
+                    f = (u32)(myrow + 1);
+                else
+                    atomicOr(&A.ctl->status, ST_OVERFLOW);
+                st_release(A.slots + idx, tagbits | genbits | f);
+                state = S_DONE;
+            }
+        }
+        // Waits on other warps' publications (bounded).
+        if (state == S_WAIT) {
+            u32 f = FIELD_PENDING;
+            for (long long s = 0; s < WAIT_SPINS; ++s) {
+                f = (u32)ld_acquire(A.slots + idx);
+                if (f != FIELD_PENDING) break;
+                __nanosleep(128);
+            }
+            if (f == FIELD_PENDING) {
+                atomicOr(&A.ctl->status, ST_WAIT);
+                state = S_DONE;
+            } else if (f == FIELD_OVERFLOW) {
+                state = S_DONE;
+            } else {
+                vrow = (long long)f - 1;
+                state = S_VERIFY;
+            }
+        }
+        // Verification of fingerprint matches.
+        if (A.key_mode == KEY_EXACT) {
+            u32 vm = __ballot_sync(FULL, state == S_VERIFY);
+            while (vm) {
+                const int t = __ffs(vm) - 1;
+                vm &= vm - 1;
+                const long long row = __shfl_sync(FULL, vrow, t);
+                const ulonglong2 *ex = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)row * A.pitch);
+                bool diff = false;
+                for (int c = lane; c < nch; c += 32) {
+                    const ulonglong2 a = g.word2(t, c);
+                    const ulonglong2 b = __ldcg(ex + c);
+                    diff |= (a.x != b.x) | (a.y != b.y);
+                }
+                const bool anydiff = __any_sync(FULL, diff);
+                if (lane == t) {
+                    if (anydiff) {
+                        state = S_PROBE;
+                        idx = (idx + 1) & A.slot_mask;
+                    } else {
+                        state = S_DONE;
+                    }
+                }
+            }
+        } else if (state == S_VERIFY) {
+            const u64 eh = __ldcg(A.keys + 2 * vrow), el = __ldcg(A.keys + 2 * vrow + 1);
+            if (eh == kh && el == kl) {
+                state = S_DONE;
+            } else {
+                state = S_PROBE;
+                idx = (idx + 1) & A.slot_mask;
+            }
+        }
+    }
+}
+
+// Fingerprints, acceptance, found flag, uniqueness for NC candidates of one warp.
+template <int NC, class Gen, class ParentOf>
+__device__ __forceinline__ void finish(const LevelArgs &A, const Gen &g, u64 (&h)[NC], u32 bad, int cnt,
+                                       ParentOf parent_of, int lane) {
+    const u64 sum = reduce_to_lane<NC>(h, lane);
+    const u32 anybad = __reduce_or_sync(FULL, bad);
+    const u32 valid = cnt >= 32 ? FULL : ((1u << cnt) - 1u);
+    const u32 acc = ~anybad & valid;
+    const u64 myparent = parent_of(lane);
+    if (acc) {
+        const int t = __ffs(acc) - 1;
+        const u64 p = __shfl_sync(FULL, myparent, t);
+        if (lane == 0) atomicCAS(&A.ctl->found, 0ull, (1ull << 63) | p);
+        if (A.stop_at_found) return;
+    }
+    if (A.check_only) return;
+    u64 fp = fmix64(sum), kh = 0, kl = 0;
+    if (A.key_mode == KEY_HASH64) {
+        kh = fp;
+    } else if (A.key_mode == KEY_REF) {
+        for (int t = 0; t < cnt; ++t) {
+            u64 a, b;
+            ref_key(A, g, t, lane, a, b);
+            if (lane == t) {
+                kh = a;
+                kl = b;
+            }
+        }
+        fp = fmix64(kh ^ fmix64(kl + 0x5ad0dedull));
+    }
+    resolve(A, g, fp, lane < cnt, myparent, kh, kl, lane);
+}
+
+__device__ __forceinline__ bool found_stop(const LevelArgs &A) {
+    return A.stop_at_found && ld_volatile(&A.ctl->found) != 0ull;
+}
+
+// ---------------------------------------------------------------- work items
+template <int OP>
+__device__ void unary_item(const LevelArgs &A, const BlockDesc &B, long long local, int warp, int nwarps, int lane,
+                           u64 &evals) {
+    const long long s_first = B.r0 + local * A.unary_rows;
+    const long long s_end = min(B.r1, s_first + (long long)A.unary_rows);
+    const int nch = A.pitch >> 1;
+    const ulonglong2 *meta = reinterpret_cast<const ulonglong2 *>(A.wmeta);
+    for (long long s = s_first + (long long)warp * UNARY_GROUP; s < s_end; s += (long long)nwarps * UNARY_GROUP) {
+        if (found_stop(A)) return;
+        const int cnt = (int)min((long long)UNARY_GROUP, s_end - s);
+        const u64 *src0 = A.cache + (u64)s * A.pitch;
+        u64 h[UNARY_GROUP];
+#pragma unroll
+        for (int t = 0; t < UNARY_GROUP; ++t) h[t] = 0;
+        u32 bad = 0;
+        u64 k = (2ull * lane + 1ull) * WEYL;
+        for (int c = lane; c < nch; c += 32, k += 64ull * WEYL) {
+            const ulonglong2 m = __ldg(meta + c);
+            const bool v0 = 2 * c < A.n, v1 = 2 * c + 1 < A.n;
+#pragma unroll
+            for (int t = 0; t < UNARY_GROUP; ++t) {
+                if (t < cnt) {
+                    const ulonglong2 sv = reinterpret_cast<const ulonglong2 *>(src0 + (size_t)t * A.pitch)[c];
+                    const u64 w0 = uop<OP>(sv.x, m.x), w1 = uop<OP>(sv.y, m.y);
+                    h[t] += hw(w0, k, v0) + hw(w1, k + WEYL, v1);
+                    bad |= badbit(w0, w1, m.x, m.y) << t;
+                }
+            }
+        }
+        UnGen<OP> g{src0, meta, A.pitch};
+        finish<UNARY_GROUP>(A, g, h, bad, cnt, [&](int t) { return pack_parent(OP, (u64)(s + t), 0); }, lane);
+        evals += (u64)cnt;
+    }
+}
+
+template <int OP, int TL>
+__device__ void binary_row(const LevelArgs &A, const ulonglong2 *tile, int nl, long long l_first, long long r,
+                           int lane, u64 &evals) {
+    constexpr int NC = OP == OP_U ? 2 * TL : TL;
+    const int nch = A.pitch >> 1;
+    const ulonglong2 *R = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)r * A.pitch);
+    const ulonglong2 *meta = reinterpret_cast<const ulonglong2 *>(A.wmeta);
+    u64 h[NC];
+#pragma unroll
+    for (int t = 0; t < NC; ++t) h[t] = 0;
+    u32 bad = 0;
+    u64 k = (2ull * lane + 1ull) * WEYL;
+    for (int c = lane; c < nch; c += 32, k += 64ull * WEYL) {
+        const ulonglong2 rv = R[c];
+        const ulonglong2 m = __ldg(meta + c);
+        const bool v0 = 2 * c < A.n, v1 = 2 * c + 1 < A.n;
+#pragma unroll
+        for (int t = 0; t < TL; ++t) {
+            if (t < nl) {
+                const ulonglong2 lv = tile[t * nch + c];
+                if (OP == OP_U) {
+                    const u64 a0 = until_bits(lv.x, rv.x), a1 = until_bits(lv.y, rv.y);
+                    const u64 b0 = until_bits(rv.x, lv.x), b1 = until_bits(rv.y, lv.y);
+                    h[2 * t] += hw(a0, k, v0) + hw(a1, k + WEYL, v1);
+                    h[2 * t + 1] += hw(b0, k, v0) + hw(b1, k + WEYL, v1);
+                    bad |= (badbit(a0, a1, m.x, m.y) << (2 * t)) | (badbit(b0, b1, m.x, m.y) << (2 * t + 1));
+                } else {
+                    const u64 w0 = bop<OP>(lv.x, rv.x), w1 = bop<OP>(lv.y, rv.y);
+                    h[t] += hw(w0, k, v0) + hw(w1, k + WEYL, v1);
+                    bad |= badbit(w0, w1, m.x, m.y) << t;
+                }
+            }
+        }
+    }
+    const int cnt = OP == OP_U ? 2 * nl : nl;
+    BinGen<OP> g{tile, R, nch};
+    finish<NC>(A, g, h, bad, cnt,
+               [&](int t) {
+                   if (OP == OP_U) {
+                       const u64 l = (u64)(l_first + (t >> 1));
+                       return (t & 1) ? pack_parent(OP, (u64)r, l) : pack_parent(OP, l, (u64)r);
+                   }
+                   return pack_parent(OP, (u64)(l_first + t), (u64)r);
+               },
+               lane);
+    evals += (u64)cnt;
+}
+
+template <int OP, int TL>
+__device__ bool binary_item(const LevelArgs &A, const BlockDesc &B, long long local, u64 *tile, u64 *bar,
+                            u32 &phase, int warp, int nwarps, int lane, u64 &evals) {
+    const long long tl = local / B.tiles_r, tr = local % B.tiles_r;
+    const long long l_first = B.l0 + tl * TL;
+    const int nl = (int)min((long long)TL, B.l1 - l_first);
+    const long long r_first = B.r0 + tr * A.right_chunk;
+    const long long r_end = min(B.r1, r_first + (long long)A.right_chunk);
+    if (threadIdx.x == 0) {
+        fence_proxy_async();
+        const u32 bytes = (u32)nl * (u32)A.pitch * 8u;
+        mbar_expect_tx(bar, bytes);
+        bulk_g2s(tile, A.cache + (u64)l_first * A.pitch, bytes, bar);
+    }
+    const bool ok = mbar_wait_bounded(bar, phase);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(&A.ctl->status, ST_TMA);
+        mbar_wait_bounded(bar, phase);  // let the copy in flight land before the CTA leaves
+        return false;
+    }
+    phase ^= 1u;
+    const ulonglong2 *t2 = reinterpret_cast<const ulonglong2 *>(tile);
+    for (long long r = r_first + warp; r < r_end; r += nwarps) {
+        if (found_stop(A)) break;
+        binary_row<OP, TL>(A, t2, nl, l_first, r, lane, evals);
+    }
+    return true;
+}
+
+template <int TL>
+__global__ void __launch_bounds__(256) level_kernel(const __grid_constant__ LevelArgs A) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    u64 *tile = reinterpret_cast<u64 *>(smem_raw);
+    __shared__ __align__(8) u64 bar;
+    __shared__ long long s_item;
+    __shared__ u64 s_evals;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        s_evals = 0;
+    }
+    __syncthreads();
+    u32 phase = 0;
+    u64 evals = 0;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            long long it = -1;
+            if (!found_stop(A)) {
+                it = (long long)atomicAdd(&A.ctl->queue_head, 1ull);
+                if (it >= A.total_items) it = -1;
+            }
+            s_item = it;
+        }
+        __syncthreads();
+        const long long item = s_item;
+        if (item < 0) break;
+        int lo = 0, hi = A.nblocks - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (A.blocks[mid].item0 <= item)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const BlockDesc B = A.blocks[lo];
+        const long long local = item - B.item0;
+        bool ok = true;
+        switch (B.op) {
+        case OP_NEG: unary_item<OP_NEG>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_X: unary_item<OP_X>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_F: unary_item<OP_F>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_G: unary_item<OP_G>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_AND: ok = binary_item<OP_AND, TL>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
+        case OP_OR: ok = binary_item<OP_OR, TL>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
+        case OP_U: ok = binary_item<OP_U, TL>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
+        default: break;
+        }
+        if (!ok) break;
+        __syncthreads();
+    }
+    if (lane == 0 && evals) atomicAdd(&s_evals, evals);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_evals) atomicAdd(&A.ctl->evaluated, s_evals);
+}
+
+// Letters: register rows [0, nalpha) in the hash set (duplicate letters stay rows,
+// as the reference stores every letter, ltli6463.cu:1134, :1189-1190).  One warp.
+__global__ void insert_letters_kernel(const __grid_constant__ LevelArgs A, int nalpha) {
+    const int lane = threadIdx.x & 31;
+    const int nch = A.pitch >> 1;
+    const ulonglong2 *meta = reinterpret_cast<const ulonglong2 *>(A.wmeta);
+    for (int j = 0; j < nalpha; ++j) {
+        const u64 *row = A.cache + (u64)j * A.pitch;
+        u64 h[1] = {0};
+        u64 k = (2ull * lane + 1ull) * WEYL;
+        for (int c = lane; c < nch; c += 32, k += 64ull * WEYL) {
+            const ulonglong2 w = reinterpret_cast<const ulonglong2 *>(row)[c];
+            h[0] += hw(w.x, k, 2 * c < A.n) + hw(w.y, k + WEYL, 2 * c + 1 < A.n);
+        }
+        (void)meta;
+        const u64 sum = reduce_to_lane<1>(h, lane);
+        u64 fp = fmix64(sum), kh = 0, kl = 0;
+        const RowGen g{reinterpret_cast<const ulonglong2 *>(row)};
+        if (A.key_mode == KEY_HASH64) {
+            kh = fp;
+        } else if (A.key_mode == KEY_REF) {
+            ref_key(A, g, 0, lane, kh, kl);
+            fp = fmix64(kh ^ fmix64(kl + 0x5ad0dedull));
+        }
+        // Probe with lane 0; a fingerprint match is verified by the whole warp.
+        const u64 tagbits = (fp >> 40) << 40, genbits = (u64)A.gen << 32;
+        u64 idx = fp & A.slot_mask;
+        for (u64 probe = 0; probe <= A.slot_mask; ++probe, idx = (idx + 1) & A.slot_mask) {
+            u64 v = 0;
+            int action = 0;  // 0 next, 1 claimed, 2 compare
+            if (lane == 0) {
+                v = ld_acquire(A.slots + idx);
+                if (slot_free(v, A.gen)) {
+                    const u64 old = atomicCAS(A.slots + idx, v, tagbits | genbits | (u64)(j + 1));
+                    if (old == v) {
+                        action = 1;
+                    } else {
+                        v = old;
+                    }
+                }
+                if (action == 0 && (v >> 40) == (tagbits >> 40) && (u32)v < FIELD_OVERFLOW) action = 2;
+            }
+            action = __shfl_sync(FULL, action, 0);
+            v = __shfl_sync(FULL, v, 0);
+            if (action == 1) {
+                if (lane == 0) {
+                    A.parents[j] = pack_parent(OP_ATOM, 0, 0);
+                    if (A.keys) {
+                        A.keys[2 * j] = kh;
+                        A.keys[2 * j + 1] = kl;
+                    }
+                }
+                break;
+            }
+            if (action == 2) {
+                const u64 other = (u64)(u32)v - 1;
+                bool same;
+                if (A.key_mode == KEY_EXACT) {
+                    bool diff = false;
+                    const ulonglong2 *ex = reinterpret_cast<const ulonglong2 *>(A.cache + other * A.pitch);
+                    for (int c = lane; c < nch; c += 32) {
+                        const ulonglong2 a = g.word2(0, c), b = __ldcg(ex + c);
+                        diff |= (a.x != b.x) | (a.y != b.y);
+                    }
+                    same = !__any_sync(FULL, diff);
+                } else {
+                    same = A.keys[2 * other] == kh && A.keys[2 * other + 1] == kl;
+                }
+                if (same) {
+                    if (lane == 0) A.parents[j] = pack_parent(OP_ATOM, 0, 0);
+                    break;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Tree of the found candidate: entries (row, parents) breadth first; entry 0 is the root
+// (row ~0).  out[0] = entries written, out[1] = 1 when the buffer was too small.
+__global__ void walk_kernel(const u64 *parents, int nalpha, u64 found, u64 *out, int cap) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    u64 *e = out + 2;
+    int count = 0, head = 0, overflow = 0;
+    e[0] = ~0ull;
+    e[1] = found & ~(1ull << 63);
+    count = 1;
+    while (head < count) {
+        const u64 p = e[2 * head + 1];
+        const int op = parent_op(p);
+        u64 kids[2] = {parent_left(p), parent_right(p)};
+        const int nk = (op == OP_AND || op == OP_OR || op == OP_U) ? 2 : (op == OP_ATOM ? 0 : 1);
+        for (int q = 0; q < nk; ++q) {
+            if (kids[q] >= (u64)nalpha) {
+                if (count >= cap) {
+                    overflow = 1;
+                    break;
+                }
+                e[2 * count] = kids[q];
+                e[2 * count + 1] = parents[kids[q]];
+                ++count;
+            }
+        }
+        ++head;
+    }
+    out[0] = (u64)count;
+    out[1] = (u64)overflow;
+}
+
+// Operator + fingerprint on independent rows, for kernel-level parity tests.  One warp per row.
+__global__ void apply_op_kernel(int op, const u64 *a, const u64 *b, const u64 *wmeta, int n, int pitch, int count,
+                                u64 *out, u64 *out2, u64 *fp) {
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= count) return;
+    u64 h1 = 0, h2 = 0;
+    for (int i = lane; i < pitch; i += 32) {
+        const u64 x = a[(u64)row * pitch + i], y = b ? b[(u64)row * pitch + i] : 0;
+        const u64 m = wmeta[i];
+        u64 w = 0, w2 = 0;
+        switch (op) {
+        case OP_NEG: w = uop<OP_NEG>(x, m); break;
+        case OP_X: w = uop<OP_X>(x, m); break;
+        case OP_F: w = uop<OP_F>(x, m); break;
+        case OP_G: w = uop<OP_G>(x, m); break;
+        case OP_AND: w = bop<OP_AND>(x, y); break;
+        case OP_OR: w = bop<OP_OR>(x, y); break;
+        case OP_U:
+            w = until_bits(x, y);
+            w2 = until_bits(y, x);
+            break;
+        default: w = x; break;
+        }
+        out[(u64)row * pitch + i] = w;
+        if (out2) out2[(u64)row * pitch + i] = w2;
+        const u64 key = (u64)(i + 1) * WEYL;
+        h1 += hw(w, key, i < n);
+        h2 += hw(w2, key, i < n);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        h1 += __shfl_xor_sync(FULL, h1, o);
+        h2 += __shfl_xor_sync(FULL, h2, o);
+    }
+    if (lane == 0) {
+        fp[row] = fmix64(h1);
+        if (out2) fp[count + row] = fmix64(h2);
+    }
+}
+
+}  // namespace
+
+int level_kernel_smem_bytes(int left_tile, int pitch) { return left_tile * pitch * 8; }
+
+int level_kernel_max_ctas_per_sm(int left_tile, int block, int smem) {
+    int n = 0;
+    cudaError_t e;
+    if (left_tile == 4)
+        cudaFuncSetAttribute(level_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    else if (left_tile == 16)
+        cudaFuncSetAttribute(level_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    else
+        cudaFuncSetAttribute(level_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (left_tile == 4)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<4>, block, smem);
+    else if (left_tile == 16)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<16>, block, smem);
+    else
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<8>, block, smem);
+    return e == cudaSuccess ? n : 0;
+}
+
+template <int TL>
+static cudaError_t launch_tl(const LevelArgs &a, int grid, int block, cudaStream_t s) {
+    const int smem = level_kernel_smem_bytes(TL, a.pitch);
+    static int attr_set = -1;  // largest dynamic shared memory size enabled so far
+    if (smem > 48 * 1024 && smem > attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(level_kernel<TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_set = smem;
+    }
+    level_kernel<TL><<<grid, block, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_level(const LevelArgs &a, int grid, int block, cudaStream_t s) {
+    if (a.left_tile == 4) return launch_tl<4>(a, grid, block, s);
+    if (a.left_tile == 16) return launch_tl<16>(a, grid, block, s);
+    return launch_tl<8>(a, grid, block, s);
+}
+
+cudaError_t launch_insert_letters(const LevelArgs &a, int nalpha, cudaStream_t s) {
+    insert_letters_kernel<<<1, 32, 0, s>>>(a, nalpha);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_walk(const u64 *parents, int nalpha, u64 found, u64 *out, int cap, cudaStream_t s) {
+    walk_kernel<<<1, 32, 0, s>>>(parents, nalpha, found, out, cap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_apply_op(int op, const u64 *a, const u64 *b, const u64 *wmeta, int n, int pitch, int count,
+                            u64 *out, u64 *out2, u64 *fp, cudaStream_t s) {
+    const int warps = 4;
+    apply_op_kernel<<<(count + warps - 1) / warps, warps * 32, 0, s>>>(op, a, b, wmeta, n, pitch, count, out, out2,
+                                                                       fp);
+    return cudaGetLastError();
+}
+
+}  // namespace ltlg

@@ -1,0 +1,66 @@
+"""The C ABI library: it loads without a GPU, exports what include/ltlgpu.h declares,
+and its host-only pieces (Scarlet reader, status strings) behave as the reference."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from ltlb200 import api, gen
+from helpers import fixture_path, load_fixture
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "ltlgpu.h")).read()
+    return sorted(set(re.findall(r"LTLG_API\s+[\w\s\*]+?\b(ltlg_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(api.LIB_PATH)
+    names = declared_symbols()
+    assert len(names) >= 14
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) == set(api.EXPORTED)
+
+
+def test_abi_version_and_status_strings():
+    lib = api.lib()
+    assert lib.ltlg_abi_version() == 1
+    assert api.status_string(api.NOT_FOUND) == "not_found"
+    assert api.status_string(api.INPUT_LIMITS) == "see_the_error"
+
+
+def test_scarlet_reader_matches_python_reader():
+    for name in ("ham1_len3.trace", "f10x10_p3_s0.trace", "cfg1_deep.trace", "len64.trace"):
+        a = api.read_scarlet(fixture_path(name))
+        b = load_fixture(name)
+        assert a.num_pos == b.num_pos and a.num_neg == b.num_neg and a.alphabet == b.alphabet
+        assert np.array_equal(a.offsets, b.offsets) and np.array_equal(a.steps, b.steps)
+
+
+def test_scarlet_reader_rules(tmp_path):
+    # file order of the letters maps values; the letter index is the sorted order;
+    # a trailing newline on the letter line is ignored; other characters advance the index
+    p = tmp_path / "t.trace"
+    p.write_text("1,0;0,1\n1,1\n---\n0,0;1 ,0\n---\nops\n---\nq,p\n")
+    t = api.read_scarlet(str(p))
+    assert t.alphabet == "pq" and t.num_pos == 2 and t.num_neg == 1
+    q, pp = 1 << (ord("q") - 97), 1 << (ord("p") - 97)
+    assert list(t.steps) == [q, pp, q | pp, 0, q]  # "1 ,0": '1' is index 0 (q), ' ' advances
+    assert list(t.offsets) == [0, 2, 3, 5]
+    u = gen.from_scarlet_text(p.read_text())
+    assert np.array_equal(u.steps, t.steps) and u.alphabet == t.alphabet
+
+
+def test_generator_is_deterministic():
+    a = gen.generate(5, 3, 50, 50, 4, 20, 0.5, 6)
+    b = gen.generate(5, 3, 50, 50, 4, 20, 0.5, 6)
+    assert np.array_equal(a.steps, b.steps) and a.hidden == b.hidden
+    h = gen.generate_hamming(3, 4, 40, 40, 20, 48, 0.5, 5)
+    assert h.num_pos == 40 and h.num_neg == 40
+    # every negative differs from every positive
+    lines = h.trace_lines()
+    assert not set(lines[:40]) & set(lines[40:])

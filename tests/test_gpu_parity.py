@@ -1,0 +1,172 @@
+"""GPU path vs the CPU oracle: per-level unique-CS sets, counts, minimal cost, formulas.
+
+All calls go through the C ABI (libltlgpu.so).  Integer work: comparisons are exact.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from ltlb200 import api, gen
+from helpers import load_fixture, lensum, row_set
+
+pytestmark = pytest.mark.gpu
+
+OPCODES = {"~": 0, "&": 1, "|": 2, "X": 3, "F": 4, "G": 5, "U": 6}
+
+
+@pytest.fixture(scope="module")
+def engine():
+    e = api.Engine(slots_log2=24, cache_bytes=4 << 30, max_rows=8 << 20)
+    yield e
+    e.close()
+
+
+def gpu_levels(engine, inst, max_cost, **kw):
+    res = engine.learn(inst, max_cost=max_cost, stop_at_found=False, **kw)
+    starts = engine.level_starts(max_cost + 2)
+    rows, par = engine.read_rows(0, starts[max_cost + 1])
+    return res, starts, rows, par
+
+
+def assert_levels_equal(inst, engine, costs, max_cost, neg_type, schedule=api.SCHEDULE_FUSED, oracle_key=O.KEY_EXACT,
+                        key_mode=api.KEY_EXACT, rlx_type=3):
+    res, starts, rows, par = gpu_levels(engine, inst, max_cost, costs=costs, neg_type=neg_type, schedule=schedule,
+                                        key_mode=key_mode, rlx_type=rlx_type)
+    assert res.device_flags & ~1 == 0, res.device_flags
+    ref = O.learn(inst, costs=costs, max_cost=max_cost, neg_type=neg_type, stop_at_found=False, key_mode=oracle_key,
+                  cache_rows=8 << 20)
+    for c in range(costs[0], max_cost + 1):
+        mine = rows[starts[c]:starts[c + 1]]
+        theirs = ref.level_rows(c)
+        assert len(mine) == len(theirs), (c, len(mine), len(theirs))
+        if key_mode == api.KEY_EXACT:
+            assert row_set(mine) == row_set(theirs), c
+    return res, ref, rows, par, starts
+
+
+def check_parents(inst, rows, par, starts, max_cost):
+    """Every stored row equals its operator applied to its parent rows."""
+    n = inst.n
+    mask = (np.uint64(1) << inst.lengths.astype(np.uint64)) - np.uint64(1)
+    nal = len(inst.alphabet)
+    for r in range(nal, starts[max_cost + 1]):
+        p = int(par[r])
+        op, l, rr = (p >> 60) & 7, (p >> 30) & 0x3FFFFFFF, p & 0x3FFFFFFF
+        out, out2 = O.apply_op(op, rows[l], rows[rr] if op in (1, 2, 6) else None, mask)
+        assert np.array_equal(out, rows[r]), (r, op, l, rr)
+    assert n == rows.shape[1]
+
+
+@pytest.mark.parametrize("name,max_cost,neg", [("ham1_len3.trace", 7, 1), ("ham1_len4.trace", 7, 2),
+                                               ("ham2_len3.trace", 7, 1), ("f10x10_p3_s0.trace", 5, 2),
+                                               ("deep8x8_p3_s508.trace", 6, 1), ("e10x2_p3_s1.trace", 6, 1)])
+def test_level_sets_fixtures(engine, name, max_cost, neg):
+    inst = load_fixture(name)
+    res, ref, rows, par, starts = assert_levels_equal(inst, engine, [1] * 8, max_cost, neg)
+    check_parents(inst, rows, par, starts, max_cost)
+
+
+@pytest.mark.parametrize("costs", [[1, 2, 1, 1, 2, 3, 3, 2], [2, 1, 3, 2, 1, 1, 2, 3]])
+def test_level_sets_skewed_costs(engine, costs):
+    inst = load_fixture("deep8x8_p3_s512.trace")
+    assert_levels_equal(inst, engine, costs, 9, 2)
+
+
+def test_level_sets_cfg1_shape(engine):
+    inst = gen.generate(450, 2, 20, 20, 8, 16, 0.5, 8)
+    assert_levels_equal(inst, engine, [1] * 8, 7, 1)
+
+
+def test_level_sets_thousand_traces(engine):
+    inst = gen.generate(2, 3, 500, 500, 16, 32, 0.5, 9)
+    assert_levels_equal(inst, engine, [1] * 8, 6, 1)
+
+
+def test_per_block_schedule_matches_oracle_progress(engine):
+    inst = load_fixture("deep8x8_p3_s530.trace")
+    res = engine.learn(inst, max_cost=7, stop_at_found=False, neg_type=1, schedule=api.SCHEDULE_PER_BLOCK)
+    ref = O.learn(inst, max_cost=7, stop_at_found=False, neg_type=1)
+    mine = [(b["cost"], b["op"], b["all_before"], b["stored_before"], b["to_check"]) for b in res.blocks]
+    theirs = [p for p in ref.progress if p[1] != "A"]
+    assert mine == theirs
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_found_cost_equals_oracle(engine, seed):
+    inst = gen.generate(seed, 2, 20, 20, 8, 16, 0.5, 5)
+    res = engine.learn(inst, neg_type=1)
+    ref = O.learn(inst, neg_type=1)
+    assert res.status == api.FOUND and ref.status == O.FOUND
+    assert res.cost == ref.cost
+    assert O.separates(res.formula, inst), res.formula
+    assert O.formula_cost(res.formula) == res.cost
+
+
+@pytest.mark.parametrize("seed", [2, 3, 8, 19])
+def test_found_cost_thousand_traces(engine, seed):
+    inst = gen.generate(seed, 3, 500, 500, 16, 32, 0.5, 9)
+    res = engine.learn(inst, neg_type=1)
+    ref = O.learn(inst, neg_type=1, threads=0, cache_rows=2 << 20, keep_rows=False)
+    assert res.cost == ref.cost
+    assert O.separates(res.formula, inst)
+    assert O.formula_cost(res.formula) == res.cost
+
+
+def test_hash64_mode_equals_exact_sets_here(engine):
+    inst = gen.generate(450, 2, 20, 20, 8, 16, 0.5, 8)
+    a = engine.learn(inst, max_cost=6, stop_at_found=False, neg_type=1, key_mode=api.KEY_HASH64)
+    ref = O.learn(inst, max_cost=6, stop_at_found=False, neg_type=1, key_mode=O.KEY_HASH64)
+    assert a.rows == ref.num_rows
+
+
+@pytest.mark.parametrize("rtype", [1, 2, 3])
+def test_reference_keys_level_counts(engine, rtype):
+    inst = gen.generate(450, 2, 20, 20, 8, 16, 0.5, 8)
+    assert lensum(inst) > 126
+    # level 2 is built only from letters, so its relaxed key set is representative-independent
+    res = engine.learn(inst, max_cost=2, stop_at_found=False, neg_type=1, key_mode=api.KEY_REF, rlx_type=rtype)
+    ref = O.learn(inst, max_cost=2, stop_at_found=False, neg_type=1, key_mode=rtype)
+    assert res.rows == ref.num_rows
+
+
+def test_device_operators_and_fingerprint_bit_exact():
+    rng = np.random.default_rng(3)
+    count, n = 50, 101
+    lens = rng.integers(1, 64, size=n)
+    mask = np.array([(1 << int(l)) - 1 for l in lens], dtype=np.uint64)
+    a = rng.integers(0, 2 ** 63, size=(count, n), dtype=np.uint64) & mask
+    b = rng.integers(0, 2 ** 63, size=(count, n), dtype=np.uint64) & mask
+    for op in range(7):
+        out, out2, fp = api.device_apply_op(op, a, b if op in (1, 2, 6) else None, mask)
+        for r in range(count):
+            o1, o2 = O.apply_op(op, a[r], b[r], mask)
+            assert np.array_equal(out[r], o1), (op, r)
+            assert int(fp[r]) == O.fp64(o1)
+            if op == 6:
+                assert np.array_equal(out2[r], o2)
+                assert int(fp[count + r]) == O.fp64(o2)
+
+
+def test_letter_hit_and_limits(engine):
+    inst = gen.generate(400, 2, 20, 20, 8, 16, 0.5, 5)  # 'p' separates
+    res = engine.learn(inst)
+    assert res.status == api.FOUND and res.cost == 1 and res.formula == "p"
+    big = load_fixture("len64.trace")
+    res = engine.learn(big)
+    assert res.status == api.INPUT_LIMITS and res.formula == "see_the_error"
+    over = load_fixture("over64.trace")
+    res = engine.learn(over, limit_traces=True)
+    assert res.status == api.INPUT_LIMITS
+    res = engine.learn(over)
+    ref = O.learn(over)
+    assert res.cost == ref.cost
+
+
+def test_engine_reuse_many_instances(engine):
+    # hash-set generations: later instances must not see earlier instances' slots
+    for seed in range(12):
+        inst = gen.generate(1000 + seed, 3, 30, 30, 5, 20, 0.5, 6)
+        res = engine.learn(inst, neg_type=1)
+        ref = O.learn(inst, neg_type=1)
+        assert res.cost == ref.cost, seed
+        assert O.separates(res.formula, inst)

@@ -446,7 +446,7 @@ __device__ void unary_item(const LevelArgs &A, const BlockDesc &B, long long loc
     const int nch = A.pitch >> 1;
     const ulonglong2 *meta = reinterpret_cast<const ulonglong2 *>(A.wmeta);
     for (long long s = s_first + (long long)warp * UNARY_GROUP; s < s_end; s += (long long)nwarps * UNARY_GROUP) {
-        if (found_stop(A)) return;
+        if (__any_sync(FULL, found_stop(A))) return;  // warp-uniform: lanes must not split
         const int cnt = (int)min((long long)UNARY_GROUP, s_end - s);
         const u64 *src0 = A.cache + (u64)s * A.pitch;
         u64 h[UNARY_GROUP];
@@ -544,7 +544,7 @@ __device__ bool binary_item(const LevelArgs &A, const BlockDesc &B, long long lo
     phase ^= 1u;
     const ulonglong2 *t2 = reinterpret_cast<const ulonglong2 *>(tile);
     for (long long r = r_first + warp; r < r_end; r += nwarps) {
-        if (found_stop(A)) break;
+        if (__any_sync(FULL, found_stop(A))) break;  // warp-uniform: lanes must not split
         binary_row<OP, TL>(A, t2, nl, l_first, r, lane, evals);
     }
     return true;

@@ -1,0 +1,319 @@
+#!/usr/bin/env python
+"""Benchmark of the characteristic-set (CS) enumeration on B200.
+
+Workload (one "step"): a fixed batch of seeded instances of the cfg2 shape — 3
+propositions, 500 positive + 500 negative traces of length uniform 16-32,
+Bernoulli(0.5) bits, labels from a hidden formula of size 9, unit costs, exact
+uniqueness in a 2^27-slot hash set — each solved to its minimal formula.
+
+Metric: unique CS per second (time-to-minimal-formula and candidate CS/s are
+reported beside it).  ``value`` divides by the device time of the level kernels
+(inputs already in HBM); ``e2e`` divides by the CUDA-event time of the whole
+public call (host traces in, formula string out) on the engine's stream.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With N > 1 (torchrun) every rank solves its own batch (weak scaling, no data-path
+collective); rank 0 prints the JSON line with the max step time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-minimal-formula & unique CS/s; learned vs plain order, same cost"
+UNIT = "unique CS/s"
+WORKLOAD = ("cfg2: 3 props, 500+500 traces, len U[16,32], Bernoulli(0.5), hidden formula size 9, unit costs, "
+            "exact uniqueness, 2^27-slot hash set; a batch of seeded instances solved to the minimal formula")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--seeds", type=str, default="0-39", help="seed range a-b of the batch (per rank)")
+    ap.add_argument("--max-cost", type=int, default=500)
+    ap.add_argument("--no-stop", action="store_true", help="enumerate every level up to --max-cost")
+    ap.add_argument("--cache-gb", type=float, default=32.0)
+    ap.add_argument("--slots-log2", type=int, default=27)
+    ap.add_argument("--cpu-sample-s", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--quiet-extra", action="store_true")
+    return ap.parse_args()
+
+
+def seeds_of(spec: str, rank: int):
+    a, b = (int(x) for x in spec.split("-"))
+    width = b - a + 1
+    return list(range(a + rank * width, b + 1 + rank * width))
+
+
+def make_batch(seeds):
+    from __graft_entry__ import load_package
+    load_package()
+    from ltlb200 import gen
+    return [gen.generate(s, 3, 500, 500, 16, 32, 0.5, 9) for s in seeds]
+
+
+def dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int, enabled: bool):
+        self.enabled = enabled
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if self.enabled:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                     "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            except OSError:
+                self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.path or not os.path.exists(self.path):
+            return None
+        sms, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxes.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sms:
+            return None
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": max(maxes), "samples": len(sms),
+                "reasons": sorted(reasons)}
+
+
+def measured_peak_gbs():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic_per_candidate():
+    """Bytes of DRAM traffic per evaluated candidate of the level kernel, from the ncu
+    summary committed under profiles/ (None when no summary exists yet)."""
+    p = os.path.join(ROOT, "profiles", "level_kernel_cfg2.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_candidate:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def cpu_baseline(batch, sample_s: float, threads: int = 0, costs=(1,) * 8):
+    """The CPU port of the same enumeration (oracle/, OpenMP) on the host cores, on the
+    batch in order until sample_s seconds are spent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    t0 = time.perf_counter()
+    uniques = cands = solved = 0
+    used = 0
+    for inst in batch:
+        left = sample_s - (time.perf_counter() - t0)
+        if left <= 0:
+            break
+        r = O.learn(inst, costs=costs, neg_type=1, threads=threads, cache_rows=4 << 20, time_limit_s=left,
+                    keep_rows=False)
+        uniques += r.num_rows - len(inst.alphabet)
+        cands += r.evaluated - len(inst.alphabet)
+        used = r.threads
+        solved += r.status == O.FOUND
+    el = time.perf_counter() - t0
+    return {"value": uniques / el, "unit": UNIT, "cores": used, "kind": "port",
+            "sample": f"{solved} of {len(batch)} batch instances solved in {el:.1f} s "
+                      f"(CPU port of the same enumeration, OpenMP, exact uniqueness)",
+            "candidate_cs_per_s": cands / el, "seconds": el}
+
+
+def run_reference(a):
+    ws, rank, local = dist()
+    if rank != 0:
+        return 0
+    batch = make_batch(seeds_of(a.seeds, 0))
+    per_step = max(5.0, min(a.cpu_sample_s, 60.0))
+    for _ in range(a.warmup):
+        cpu_baseline(batch[:1], per_step / 4)
+    vals, secs = [], []
+    last = None
+    for _ in range(a.steps):
+        last = cpu_baseline(batch, per_step)
+        vals.append(last["value"])
+        secs.append(last["seconds"])
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * statistics.median(secs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "seeds": a.seeds, "parallelism": "cpu"},
+            "cpu_baseline": {**last, "value": value},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(a):
+    import torch
+    ws, rank, local = dist()
+    if ws > 1:
+        import torch.distributed as D
+        D.init_process_group(backend="nccl", timeout=datetime.timedelta(seconds=300),
+                             device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    from __graft_entry__ import load_package
+    load_package()
+    from ltlb200 import api
+    batch = make_batch(seeds_of(a.seeds, rank))
+    eng = api.Engine(device=local, slots_log2=a.slots_log2, cache_bytes=int(a.cache_gb * (1 << 30)))
+    stream = torch.cuda.ExternalStream(eng.stream, device=torch.device("cuda", local))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    opts = dict(neg_type=1, max_cost=a.max_cost, stop_at_found=not a.no_stop)
+
+    def step():
+        return [eng.learn(inst, **opts) for inst in batch]
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as D
+            D.barrier()
+
+    step_ms, kern_ms, uniques, cands, launches, ttm, costs = [], [], 0, 0, 0, [], []
+    h2d = d2h = 0
+    with Clocks(local, enabled=not a.no_clocks) as clk:
+        for _ in range(a.steps):
+            flush.fill_(1)  # L2 flush between timed steps (256 MiB write)
+            torch.cuda.synchronize()
+            barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            res = step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            step_ms.append(e0.elapsed_time(e1))
+            kern_ms.append(sum(r.device_ms for r in res))
+            for inst, r in zip(batch, res):
+                assert r.status == api.FOUND or a.no_stop, (r.status, r.formula)
+                uniques += r.rows - len(inst.alphabet)
+                cands += r.evaluated - len(inst.alphabet)
+                launches += r.launches
+                ttm.append(r.seconds * 1e3)
+                costs.append(r.cost)
+                h2d += len(inst.alphabet) * inst.n * 8 + inst.n * 12  # letter CSs + word metadata
+                d2h += len(r.formula) + 64
+    clocks = clk.summary()
+    K = a.steps
+    step_t = sum(step_ms) / 1e3
+    kern_t = sum(kern_ms) / 1e3
+    n = batch[0].n
+    if ws > 1:
+        import torch.distributed as D
+        t = torch.tensor([step_t, kern_t], dtype=torch.float64, device="cuda")
+        D.all_reduce(t, op=D.ReduceOp.MAX)
+        u = torch.tensor([uniques, cands], dtype=torch.float64, device="cuda")
+        D.all_reduce(u, op=D.ReduceOp.SUM)
+        step_t, kern_t = float(t[0]), float(t[1])
+        uniques_all, cands_all = float(u[0]), float(u[1])
+    else:
+        uniques_all, cands_all = float(uniques), float(cands)
+    if rank == 0:
+        peak, peak_kind = measured_peak_gbs()
+        per_unit = 8 * n + 8
+        alg_bytes = (cands + uniques) * per_unit  # this rank's bytes over its own kernel time
+        achieved = alg_bytes / (sum(kern_ms) / 1e3) / 1e9
+        level_launches = max(1, launches - K * len(batch) * 2)
+        tpc = profile_traffic_per_candidate()
+        line = {
+            "metric": METRIC, "value": uniques_all / kern_t, "unit": UNIT, "n_gpus": ws, "steps": K,
+            "warmup": a.warmup, "ms_per_step": 1e3 * step_t / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "seeds_per_rank": a.seeds, "instances_per_step": len(batch) * ws,
+                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"instances x{ws} ranks"},
+            "time_to_minimal_formula_ms": {"mean": statistics.mean(ttm), "median": statistics.median(ttm),
+                                           "max": max(ttm), "min_cost": min(costs), "max_cost": max(costs)},
+            "candidate_cs_per_s": cands_all / kern_t,
+            "e2e": {"value": uniques_all / step_t, "unit": UNIT, "h2d_bytes_per_step": h2d // K,
+                    "d2h_bytes_per_step": d2h // K, "candidate_cs_per_s": cands_all / step_t},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": (tpc * cands / level_launches) if tpc else None,
+                         "kernel": "level_kernel", "bytes_per_unit": per_unit,
+                         "units": "candidates evaluated + uniques stored"},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        if ws == 1 and not a.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(batch, a.cpu_sample_s)
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if ws > 1:
+        import torch.distributed as D
+        D.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

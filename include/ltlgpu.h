@@ -138,7 +138,7 @@ typedef struct ltlg_result {
     int32_t found_op;          /* root operator of the returned formula (7 for a letter) */
     uint32_t device_flags;     /* raw device status bits (overflow, waits, table) */
     int32_t on_the_fly;        /* 1 once the cache overflowed (the reference's onTheFly) */
-    int32_t pad_;
+    int32_t launches;          /* kernels this call launched */
 } ltlg_result;
 
 typedef struct ltlg_engine ltlg_engine;
@@ -154,6 +154,10 @@ LTLG_API void ltlg_engine_destroy(ltlg_engine *eng);
 /* Learn one formula.  Replaces LTLI (ltli6463.cu:1043); the engine's buffers are reused. */
 LTLG_API int ltlg_engine_learn(ltlg_engine *eng, const ltlg_traces *traces, const ltlg_options *opt,
                                ltlg_result *res);
+
+/* The engine's CUDA stream (a cudaStream_t), for callers that time or order work around
+ * learns with their own events. */
+LTLG_API void *ltlg_engine_stream(ltlg_engine *eng);
 
 /* One-shot form: creates an engine sized for the input, learns, destroys it. */
 LTLG_API int ltlg_learn(const ltlg_traces *traces, const ltlg_options *opt, ltlg_result *res);

@@ -28,7 +28,7 @@ EXPORTED = [
     "ltlg_abi_version", "ltlg_status_string", "ltlg_default_engine_config", "ltlg_default_options",
     "ltlg_engine_create", "ltlg_engine_destroy", "ltlg_engine_learn", "ltlg_learn", "ltlg_result_free",
     "ltlg_engine_read_rows", "ltlg_engine_level_starts", "ltlg_device_apply_op", "ltlg_read_scarlet",
-    "ltlg_traces_free",
+    "ltlg_traces_free", "ltlg_engine_stream",
 ]
 
 
@@ -66,7 +66,7 @@ class Result(C.Structure):
                 ("rows", C.c_int64), ("formula", C.c_void_p), ("seconds", C.c_double), ("device_ms", C.c_double),
                 ("num_levels", C.c_int32), ("num_blocks", C.c_int32), ("levels", C.POINTER(LevelStat)),
                 ("blocks", C.POINTER(BlockStat)), ("found_op", C.c_int32), ("device_flags", C.c_uint32),
-                ("on_the_fly", C.c_int32), ("pad_", C.c_int32)]
+                ("on_the_fly", C.c_int32), ("launches", C.c_int32)]
 
 
 _lib = None
@@ -95,6 +95,8 @@ def lib():
                                            C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.ltlg_read_scarlet.argtypes = [C.c_char_p, C.POINTER(Traces)]
         L.ltlg_traces_free.argtypes = [C.POINTER(Traces)]
+        L.ltlg_engine_stream.argtypes = [C.c_void_p]
+        L.ltlg_engine_stream.restype = C.c_void_p
         _lib = L
     return _lib
 
@@ -131,6 +133,7 @@ class LearnResult:
     found_op: int
     device_flags: int
     on_the_fly: bool
+    launches: int
 
     @property
     def found(self) -> bool:
@@ -145,7 +148,7 @@ def _result(r: Result) -> LearnResult:
               for b in (r.blocks[i] for i in range(r.num_blocks))]
     return LearnResult(r.status, r.cost, r.all_ltls, r.evaluated, r.rows,
                        C.string_at(r.formula).decode() if r.formula else "", r.seconds, r.device_ms, levels, blocks,
-                       r.found_op, r.device_flags, bool(r.on_the_fly))
+                       r.found_op, r.device_flags, bool(r.on_the_fly), r.launches)
 
 
 def make_options(costs=(1,) * 8, max_cost=500, rlx_type=3, neg_type=2, key_mode=KEY_EXACT,
@@ -215,6 +218,11 @@ class Engine:
             lib().ltlg_result_free(C.byref(r))
         self.n = inst.n
         return out
+
+    @property
+    def stream(self) -> int:
+        """The engine's cudaStream_t as an integer handle."""
+        return lib().ltlg_engine_stream(self._h) or 0
 
     def level_starts(self, count: int) -> list:
         a = (C.c_int64 * count)()

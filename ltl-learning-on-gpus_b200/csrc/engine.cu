@@ -455,6 +455,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     }
     A.left_tile = tl;
     if ((err = launch_insert_letters(A, nalpha, st)) != cudaSuccess) return fail_cuda(e, err, res);
+    int launches = 1;
 
     const int block_threads = e->cfg.block_threads;
     const int smem = level_kernel_smem_bytes(tl, pitch);
@@ -494,6 +495,19 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         BlockDesc *hb = (BlockDesc *)e->h_blocks.p;
         long long items = 0;
         uint64_t level_cands = 0;
+        for (const Block &B : blocks) level_cands += (uint64_t)B.candidates;
+        // Work-item size: a small level is cut into one right row (or one group of source
+        // rows) per warp so every SM takes part; a large level keeps the configured sizes.
+        {
+            const int nwarps = block_threads / 32;
+            if ((long long)level_cands < max_grid * 2048ll) {
+                A.right_chunk = nwarps;
+                A.unary_rows = nwarps * 4;
+            } else {
+                A.right_chunk = e->cfg.right_chunk;
+                A.unary_rows = e->cfg.unary_rows;
+            }
+        }
         for (size_t b = 0; b < nb; ++b) {
             const Block &B = blocks[b];
             BlockDesc d{};
@@ -512,20 +526,20 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
             }
             items += d.items;
             hb[b] = d;
-            level_cands += (uint64_t)B.candidates;
         }
         const long long stored_before = ls[cost];
         if (nb) cudaMemcpyAsync(e->blocks.p, hb, nb * sizeof(BlockDesc), cudaMemcpyHostToDevice, st);
         A.blocks = (const BlockDesc *)e->blocks.p;
         A.check_only = on_the_fly ? 1 : 0;
+        if (!per_block && items > 0) cudaMemsetAsync(&((DevCtl *)e->ctl.p)->queue_head, 0, sizeof(u64), st);
         cudaEventRecord(e->ev_a, st);
         if (!per_block) {
             if (items > 0) {
-                cudaMemsetAsync(&((DevCtl *)e->ctl.p)->queue_head, 0, sizeof(u64), st);
                 A.nblocks = (int)nb;
                 A.total_items = items;
                 const int grid = (int)std::min<long long>(items, max_grid);
                 if ((err = launch_level(A, grid, block_threads, st)) != cudaSuccess) return fail_cuda(e, err, res);
+                ++launches;
             }
         } else {
             for (size_t b = 0; b < nb; ++b) {
@@ -539,6 +553,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
                 A.total_items = hb[b].item0 + hb[b].items;
                 const int grid = (int)std::min<long long>(hb[b].items, max_grid);
                 if ((err = launch_level(A, grid, block_threads, st)) != cudaSuccess) return fail_cuda(e, err, res);
+                ++launches;
             }
         }
         cudaEventRecord(e->ev_b, st);
@@ -553,6 +568,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         const long long stored = std::min<long long>((long long)hc->row_count, cap_rows);
         // Reference-style candidate counting: whole blocks up to the one holding the find.
         uint64_t counted = level_cands;
+        size_t nb_reported = nb;
         if (hc->found && !found) {
             const u64 p = hc->found & ~(1ull << 63);
             const int fop = parent_op(p);
@@ -560,15 +576,17 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
             int lc = cost_of_row(ls, l);
             if (fop == OP_U) lc = std::min(lc, cost_of_row(ls, r));
             counted = 0;
+            nb_reported = 0;
             for (const Block &B : blocks) {
                 counted += (uint64_t)B.candidates;
+                ++nb_reported;
                 if (B.op == fop && B.lcost == lc) break;
             }
         }
         if (per_block) {
             const DevCtl *sn = (const DevCtl *)e->h_snaps.p;
             uint64_t before = all;
-            for (size_t b = 0; b < nb; ++b) {
+            for (size_t b = 0; b < nb_reported; ++b) {
                 ltlg_block_stat s{};
                 s.cost = cost;
                 s.op = blocks[b].op;
@@ -641,6 +659,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         if ((err = launch_walk((const u64 *)e->parents.p, nalpha, found_word, (u64 *)e->walk.p, cap, st)) !=
             cudaSuccess)
             return fail_cuda(e, err, res);
+        ++launches;
         cudaMemcpyAsync(e->h_walk.p, e->walk.p, (2 + 2 * cap) * 8, cudaMemcpyDeviceToHost, st);
         if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
         const u64 *w = (const u64 *)e->h_walk.p;
@@ -667,10 +686,13 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         res->blocks = (ltlg_block_stat *)malloc(sizeof(ltlg_block_stat) * bstats.size());
         memcpy(res->blocks, bstats.data(), sizeof(ltlg_block_stat) * bstats.size());
     }
+    res->launches = launches;
     res->seconds = now_s() - t0;
     (void)OPCH;
     return res->status;
 }
+
+LTLG_API void *ltlg_engine_stream(ltlg_engine *e) { return e ? (void *)e->stream : nullptr; }
 
 LTLG_API int ltlg_learn(const ltlg_traces *t, const ltlg_options *opt, ltlg_result *res) {
     ltlg_engine_config cfg;

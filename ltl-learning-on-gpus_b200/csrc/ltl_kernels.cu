@@ -44,30 +44,30 @@ __device__ __forceinline__ u64 fmix64(u64 x) {
     return x;
 }
 
-__device__ __forceinline__ u64 smear(u64 w) {
-    w |= w >> 1;
-    w |= w >> 2;
-    w |= w >> 4;
-    w |= w >> 8;
-    w |= w >> 16;
-    w |= w >> 32;
-    return w;
+// F: every position at or before the last one where the operand holds, i.e. the
+// reference's right smear (ltli6463.cu:553-555) as (2 << msb) - 1.
+__device__ __forceinline__ u64 fin_bits(u64 w) { return w ? ((2ull << (63 - __clzll(w))) - 1ull) : 0ull; }
+
+// G: positions after the last position (inside the trace) where the operand fails,
+// ltli6463.cu:640-644 (w & ~smear(~w & mask)).  Bit 63 of a mask is never set.
+__device__ __forceinline__ u64 glob_bits(u64 w, u64 m) {
+    const u64 z = ~w & m;
+    return z ? (w & (~0ull << (64 - __clzll(z)))) : w;
 }
 
-// x U y: y holds, or x holds and (x U y) holds one step later; log-step doubling.
+// x U y.  r_k = y_k | (x_k & r_{k+1}) is a carry chain running from late to early
+// positions; bit-reversed it runs upwards, so one 64-bit addition propagates it:
+// with A = x|y and B = y (reversed), generate = A&B = y and propagate = A^B = x&~y, and
+// the carry into bit j+1 is r at reversed position j.  Positions 0..62 are reversed into
+// bits 62..0 (bit 63 of every CS is 0) so the carry into bit 63 holds position 0.  Same
+// result as the doubling recurrence of ltli6463.cu:739-752.
+__device__ __forceinline__ u64 rev62(u64 v) { return __brevll(v) >> 1; }
+__device__ __forceinline__ u64 until_rev(u64 a, u64 yr) {  // a = xr | yr
+    return __brevll(((a + yr) ^ a ^ yr) & ~1ull);
+}
 __device__ __forceinline__ u64 until_bits(u64 x, u64 y) {
-    y |= x & (y >> 1);
-    x &= x >> 1;
-    y |= x & (y >> 2);
-    x &= x >> 2;
-    y |= x & (y >> 4);
-    x &= x >> 4;
-    y |= x & (y >> 8);
-    x &= x >> 8;
-    y |= x & (y >> 16);
-    x &= x >> 16;
-    y |= x & (y >> 32);
-    return y;
+    const u64 xr = rev62(x), yr = rev62(y);
+    return until_rev(xr | yr, yr);
 }
 
 template <int OP>
@@ -75,8 +75,8 @@ __device__ __forceinline__ u64 uop(u64 w, u64 meta) {
     const u64 m = meta & LENMASK;
     if (OP == OP_NEG) return ~w & m;
     if (OP == OP_X) return w >> 1;
-    if (OP == OP_F) return smear(w);
-    return w & ~smear(~w & m);  // OP_G
+    if (OP == OP_F) return fin_bits(w);
+    return glob_bits(w, m);  // OP_G
 }
 
 template <int OP>
@@ -86,8 +86,15 @@ __device__ __forceinline__ u64 bop(u64 a, u64 b) {
     return until_bits(a, b);
 }
 
-// Word i of a CS contributes fmix64(w ^ (i + 1) * WEYL) to the fingerprint sum.
-__device__ __forceinline__ u64 hw(u64 w, u64 key, bool valid) { return valid ? fmix64(w ^ key) : 0ull; }
+// Word i (key = (i + 1) * WEYL) of a CS adds to the fingerprint sum:
+//   HK 0 (exact keys, verified): (lo(w) + lo(key)) * (hi(w) + hi(key)), one 32x32->64
+//        multiply-add in the style of the NH hash (Black et al., UMAC, 1999);
+//   HK 1 (64-bit fingerprint, not verified): fmix64(w ^ key), padding words excluded.
+template <int HK>
+__device__ __forceinline__ u64 hw(u64 w, u64 key, bool valid) {
+    if (HK == 0) return (u64)((u32)w + (u32)key) * (u64)((u32)(w >> 32) + (u32)(key >> 32));
+    return valid ? fmix64(w ^ key) : 0ull;
+}
 // Bit 0 disagrees with the label (positives need 1, negatives 0); padding words are 0 with label 0.
 __device__ __forceinline__ u32 badbit(u64 w0, u64 w1, u64 m0, u64 m1) {
     return (u32)(((w0 ^ (m0 >> 63)) | (w1 ^ (m1 >> 63))) & 1ull);
@@ -166,18 +173,20 @@ __device__ __forceinline__ u64 reduce_to_lane(u64 (&v)[NC], int lane) {
 }
 
 // ---------------------------------------------------------------- candidate generators
-// word2(t, c) recomputes words 2c, 2c+1 of candidate t.
+// pre(c) loads the operand chunk every candidate of the batch shares (binary: the right
+// row; unary: the word metadata); word(t, c, pre) gives words 2c, 2c+1 of candidate t.
 template <int OP>
 struct BinGen {
     const ulonglong2 *left;   // shared-memory tile, row stride nch
     const ulonglong2 *right;  // global right row
     int nch;
-    __device__ __forceinline__ ulonglong2 word2(int t, int c) const {
-        const ulonglong2 r = right[c];
+    __device__ __forceinline__ ulonglong2 pre(int c) const { return right[c]; }
+    __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 r) const {
         if (OP == OP_U) {
             const ulonglong2 l = left[(t >> 1) * nch + c];
-            if (t & 1) return make_ulonglong2(until_bits(r.x, l.x), until_bits(r.y, l.y));
-            return make_ulonglong2(until_bits(l.x, r.x), until_bits(l.y, r.y));
+            const u64 lx = rev62(l.x), ly = rev62(l.y), rx = rev62(r.x), ry = rev62(r.y);
+            if (t & 1) return make_ulonglong2(until_rev(lx | rx, lx), until_rev(ly | ry, ly));
+            return make_ulonglong2(until_rev(lx | rx, rx), until_rev(ly | ry, ry));
         }
         const ulonglong2 l = left[t * nch + c];
         return make_ulonglong2(bop<OP>(l.x, r.x), bop<OP>(l.y, r.y));
@@ -189,9 +198,9 @@ struct UnGen {
     const u64 *src0;  // first source row of the group; rows are consecutive
     const ulonglong2 *meta;
     int pitch;
-    __device__ __forceinline__ ulonglong2 word2(int t, int c) const {
+    __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldg(meta + c); }
+    __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 m) const {
         const ulonglong2 s = reinterpret_cast<const ulonglong2 *>(src0 + (size_t)t * pitch)[c];
-        const ulonglong2 m = __ldg(meta + c);
         return make_ulonglong2(uop<OP>(s.x, m.x), uop<OP>(s.y, m.y));
     }
 };
@@ -199,7 +208,8 @@ struct UnGen {
 // A stored row as its own candidate (letters).
 struct RowGen {
     const ulonglong2 *r;
-    __device__ __forceinline__ ulonglong2 word2(int, int c) const { return r[c]; }
+    __device__ __forceinline__ ulonglong2 pre(int c) const { return r[c]; }
+    __device__ __forceinline__ ulonglong2 word(int, int, ulonglong2 p) const { return p; }
 };
 
 // Relaxed key of candidate t (KEY_REF), warp-cooperative; result valid in every lane.
@@ -208,7 +218,7 @@ __device__ void ref_key(const LevelArgs &A, const Gen &g, int t, int lane, u64 &
     const int nch = A.pitch >> 1;
     u64 h = 0, l = 0;
     for (int c = lane; c < nch; c += 32) {
-        const ulonglong2 w2 = g.word2(t, c);
+        const ulonglong2 w2 = g.word(t, c, g.pre(c));
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
             const int i = 2 * c + e;
@@ -261,14 +271,17 @@ enum { S_DONE = 0, S_PROBE = 1, S_CLAIM = 2, S_WAIT = 3, S_VERIFY = 4 };
 
 __device__ __forceinline__ bool slot_free(u64 v, u32 gen) { return v == 0 || (u32)((v >> 32) & 0xFFu) != gen; }
 
-// Lane t owns candidate t (t < NC).  Claims are written and published before any
-// lane of the warp waits on another warp's publication, so waits cannot cycle.
-template <class Gen>
+// Lane t owns candidate t (t < NC).  Every phase that touches whole CSs (writing the
+// claimed rows, verifying fingerprint matches) is one chunk-major sweep over all the
+// candidates concerned, so their loads are in flight together.  Claims are written and
+// published before any lane waits on another warp's publication, so waits cannot cycle.
+template <int NC, class Gen>
 __device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u64 parent, u64 kh, u64 kl,
                         int lane) {
     int state = active ? S_PROBE : S_DONE;
     const u64 tagbits = (fp >> 40) << 40;
     const u64 genbits = (u64)A.gen << 32;
+    const u64 want = tagbits | genbits | FIELD_PENDING;
     u64 idx = fp & A.slot_mask;
     long long vrow = -1;
     u64 probes = 0;
@@ -277,9 +290,15 @@ __device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u
         if (state == S_PROBE) {
             for (;;) {
                 u64 *sp = A.slots + idx;
-                u64 v = ld_acquire(sp);
-                if (slot_free(v, A.gen)) {
-                    const u64 old = atomicCAS(sp, v, tagbits | genbits | FIELD_PENDING);
+                // CAS first: an empty slot is claimed in one round trip; otherwise the
+                // returned value is the slot's content.
+                u64 v = atomicCAS(sp, 0ull, want);
+                if (v == 0ull) {
+                    state = S_CLAIM;
+                    break;
+                }
+                if (slot_free(v, A.gen)) {  // a slot of an older generation
+                    const u64 old = atomicCAS(sp, v, want);
                     if (old == v) {
                         state = S_CLAIM;
                         break;
@@ -309,25 +328,27 @@ __device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u
                 }
             }
         }
-        // Claims: reserve rows (one atomic per warp), write the CSs, publish.
+        // Claims: one row reservation per warp, one sweep writing every claimed CS, publish.
         const u32 cm = __ballot_sync(FULL, state == S_CLAIM);
         if (cm) {
             const int leader = __ffs(cm) - 1;
             u64 base = 0;
             if (lane == leader) base = atomicAdd(&A.ctl->row_count, (u64)__popc(cm));
             base = __shfl_sync(FULL, base, leader);
-            u32 rem = cm;
-            while (rem) {
-                const int t = __ffs(rem) - 1;
-                rem &= rem - 1;
-                const u64 row = base + __popc(cm & ((1u << t) - 1));
-                if (row < (u64)A.cap_rows) {
-                    ulonglong2 *dst = reinterpret_cast<ulonglong2 *>(A.cache + row * (u64)A.pitch);
-                    for (int c = lane; c < nch; c += 32) dst[c] = g.word2(t, c);
+            const u64 cap = (u64)A.cap_rows;
+#pragma unroll 2
+            for (int c = lane; c < nch; c += 32) {
+                const ulonglong2 p = g.pre(c);
+#pragma unroll
+                for (int t = 0; t < NC; ++t) {
+                    if ((cm >> t) & 1u) {
+                        const u64 row = base + __popc(cm & ((1u << t) - 1u));
+                        if (row < cap) reinterpret_cast<ulonglong2 *>(A.cache + row * (u64)A.pitch)[c] = g.word(t, c, p);
+                    }
                 }
             }
-            u64 myrow = base + __popc(cm & ((1u << lane) - 1));
-            if (state == S_CLAIM && myrow < (u64)A.cap_rows) {
+            const u64 myrow = base + __popc(cm & ((1u << lane) - 1u));
+            if (state == S_CLAIM && myrow < cap) {
                 A.parents[myrow] = parent;
                 if (A.keys) {
                     A.keys[2 * myrow] = kh;
@@ -338,7 +359,7 @@ __device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u
             __syncwarp();
             if (state == S_CLAIM) {
                 u32 f = FIELD_OVERFLOW;
-                if (myrow < (u64)A.cap_rows)
+                if (myrow < cap)
                     f = (u32)(myrow + 1);
                 else
                     atomicOr(&A.ctl->status, ST_OVERFLOW);
@@ -364,23 +385,30 @@ __device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u
                 state = S_VERIFY;
             }
         }
-        // Verification of fingerprint matches.
+        // Verification of fingerprint matches: one sweep comparing every candidate with its row.
         if (A.key_mode == KEY_EXACT) {
-            u32 vm = __ballot_sync(FULL, state == S_VERIFY);
-            while (vm) {
-                const int t = __ffs(vm) - 1;
-                vm &= vm - 1;
-                const long long row = __shfl_sync(FULL, vrow, t);
-                const ulonglong2 *ex = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)row * A.pitch);
-                bool diff = false;
+            const u32 vm = __ballot_sync(FULL, state == S_VERIFY);
+            if (vm) {
+                u32 vr[NC];
+#pragma unroll
+                for (int t = 0; t < NC; ++t) vr[t] = (u32)__shfl_sync(FULL, (u32)vrow, t);
+                u32 diff = 0;
+#pragma unroll 2
                 for (int c = lane; c < nch; c += 32) {
-                    const ulonglong2 a = g.word2(t, c);
-                    const ulonglong2 b = __ldcg(ex + c);
-                    diff |= (a.x != b.x) | (a.y != b.y);
+                    const ulonglong2 p = g.pre(c);
+#pragma unroll
+                    for (int t = 0; t < NC; ++t) {
+                        if ((vm >> t) & 1u) {
+                            const ulonglong2 a = g.word(t, c, p);
+                            const ulonglong2 b = __ldcg(reinterpret_cast<const ulonglong2 *>(
+                                                            A.cache + (u64)vr[t] * (u64)A.pitch) + c);
+                            diff |= (u32)((a.x != b.x) | (a.y != b.y)) << t;
+                        }
+                    }
                 }
-                const bool anydiff = __any_sync(FULL, diff);
-                if (lane == t) {
-                    if (anydiff) {
+                const u32 anydiff = __reduce_or_sync(FULL, diff);
+                if (state == S_VERIFY) {
+                    if ((anydiff >> lane) & 1u) {
                         state = S_PROBE;
                         idx = (idx + 1) & A.slot_mask;
                     } else {
@@ -430,7 +458,7 @@ __device__ __forceinline__ void finish(const LevelArgs &A, const Gen &g, u64 (&h
         }
         fp = fmix64(kh ^ fmix64(kl + 0x5ad0dedull));
     }
-    resolve(A, g, fp, lane < cnt, myparent, kh, kl, lane);
+    resolve<NC>(A, g, fp, lane < cnt, myparent, kh, kl, lane);
 }
 
 __device__ __forceinline__ bool found_stop(const LevelArgs &A) {
@@ -438,7 +466,7 @@ __device__ __forceinline__ bool found_stop(const LevelArgs &A) {
 }
 
 // ---------------------------------------------------------------- work items
-template <int OP>
+template <int OP, int HK>
 __device__ void unary_item(const LevelArgs &A, const BlockDesc &B, long long local, int warp, int nwarps, int lane,
                            u64 &evals) {
     const long long s_first = B.r0 + local * A.unary_rows;
@@ -462,7 +490,7 @@ __device__ void unary_item(const LevelArgs &A, const BlockDesc &B, long long loc
                 if (t < cnt) {
                     const ulonglong2 sv = reinterpret_cast<const ulonglong2 *>(src0 + (size_t)t * A.pitch)[c];
                     const u64 w0 = uop<OP>(sv.x, m.x), w1 = uop<OP>(sv.y, m.y);
-                    h[t] += hw(w0, k, v0) + hw(w1, k + WEYL, v1);
+                    h[t] += hw<HK>(w0, k, v0) + hw<HK>(w1, k + WEYL, v1);
                     bad |= badbit(w0, w1, m.x, m.y) << t;
                 }
             }
@@ -473,7 +501,7 @@ __device__ void unary_item(const LevelArgs &A, const BlockDesc &B, long long loc
     }
 }
 
-template <int OP, int TL>
+template <int OP, int TL, int HK>
 __device__ void binary_row(const LevelArgs &A, const ulonglong2 *tile, int nl, long long l_first, long long r,
                            int lane, u64 &evals) {
     constexpr int NC = OP == OP_U ? 2 * TL : TL;
@@ -485,23 +513,27 @@ __device__ void binary_row(const LevelArgs &A, const ulonglong2 *tile, int nl, l
     for (int t = 0; t < NC; ++t) h[t] = 0;
     u32 bad = 0;
     u64 k = (2ull * lane + 1ull) * WEYL;
+#pragma unroll 2
     for (int c = lane; c < nch; c += 32, k += 64ull * WEYL) {
         const ulonglong2 rv = R[c];
         const ulonglong2 m = __ldg(meta + c);
         const bool v0 = 2 * c < A.n, v1 = 2 * c + 1 < A.n;
+        const u64 rx = OP == OP_U ? rev62(rv.x) : 0ull, ry = OP == OP_U ? rev62(rv.y) : 0ull;
 #pragma unroll
         for (int t = 0; t < TL; ++t) {
             if (t < nl) {
                 const ulonglong2 lv = tile[t * nch + c];
                 if (OP == OP_U) {
-                    const u64 a0 = until_bits(lv.x, rv.x), a1 = until_bits(lv.y, rv.y);
-                    const u64 b0 = until_bits(rv.x, lv.x), b1 = until_bits(rv.y, lv.y);
-                    h[2 * t] += hw(a0, k, v0) + hw(a1, k + WEYL, v1);
-                    h[2 * t + 1] += hw(b0, k, v0) + hw(b1, k + WEYL, v1);
+                    const u64 lx = rev62(lv.x), ly = rev62(lv.y);
+                    const u64 ax = lx | rx, ay = ly | ry;
+                    const u64 a0 = until_rev(ax, rx), a1 = until_rev(ay, ry);  // l U r
+                    const u64 b0 = until_rev(ax, lx), b1 = until_rev(ay, ly);  // r U l
+                    h[2 * t] += hw<HK>(a0, k, v0) + hw<HK>(a1, k + WEYL, v1);
+                    h[2 * t + 1] += hw<HK>(b0, k, v0) + hw<HK>(b1, k + WEYL, v1);
                     bad |= (badbit(a0, a1, m.x, m.y) << (2 * t)) | (badbit(b0, b1, m.x, m.y) << (2 * t + 1));
                 } else {
                     const u64 w0 = bop<OP>(lv.x, rv.x), w1 = bop<OP>(lv.y, rv.y);
-                    h[t] += hw(w0, k, v0) + hw(w1, k + WEYL, v1);
+                    h[t] += hw<HK>(w0, k, v0) + hw<HK>(w1, k + WEYL, v1);
                     bad |= badbit(w0, w1, m.x, m.y) << t;
                 }
             }
@@ -521,7 +553,7 @@ __device__ void binary_row(const LevelArgs &A, const ulonglong2 *tile, int nl, l
     evals += (u64)cnt;
 }
 
-template <int OP, int TL>
+template <int OP, int TL, int HK>
 __device__ bool binary_item(const LevelArgs &A, const BlockDesc &B, long long local, u64 *tile, u64 *bar,
                             u32 &phase, int warp, int nwarps, int lane, u64 &evals) {
     const long long tl = local / B.tiles_r, tr = local % B.tiles_r;
@@ -545,13 +577,13 @@ __device__ bool binary_item(const LevelArgs &A, const BlockDesc &B, long long lo
     const ulonglong2 *t2 = reinterpret_cast<const ulonglong2 *>(tile);
     for (long long r = r_first + warp; r < r_end; r += nwarps) {
         if (__any_sync(FULL, found_stop(A))) break;  // warp-uniform: lanes must not split
-        binary_row<OP, TL>(A, t2, nl, l_first, r, lane, evals);
+        binary_row<OP, TL, HK>(A, t2, nl, l_first, r, lane, evals);
     }
     return true;
 }
 
-template <int TL>
-__global__ void __launch_bounds__(256) level_kernel(const __grid_constant__ LevelArgs A) {
+template <int TL, int HK>
+__global__ void __launch_bounds__(256, 3) level_kernel(const __grid_constant__ LevelArgs A) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     u64 *tile = reinterpret_cast<u64 *>(smem_raw);
     __shared__ __align__(8) u64 bar;
@@ -590,13 +622,13 @@ __global__ void __launch_bounds__(256) level_kernel(const __grid_constant__ Leve
         const long long local = item - B.item0;
         bool ok = true;
         switch (B.op) {
-        case OP_NEG: unary_item<OP_NEG>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_X: unary_item<OP_X>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_F: unary_item<OP_F>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_G: unary_item<OP_G>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_AND: ok = binary_item<OP_AND, TL>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
-        case OP_OR: ok = binary_item<OP_OR, TL>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
-        case OP_U: ok = binary_item<OP_U, TL>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
+        case OP_NEG: unary_item<OP_NEG, HK>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_X: unary_item<OP_X, HK>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_F: unary_item<OP_F, HK>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_G: unary_item<OP_G, HK>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_AND: ok = binary_item<OP_AND, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
+        case OP_OR: ok = binary_item<OP_OR, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
+        case OP_U: ok = binary_item<OP_U, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
         default: break;
         }
         if (!ok) break;
@@ -609,6 +641,7 @@ __global__ void __launch_bounds__(256) level_kernel(const __grid_constant__ Leve
 
 // Letters: register rows [0, nalpha) in the hash set (duplicate letters stay rows,
 // as the reference stores every letter, ltli6463.cu:1134, :1189-1190).  One warp.
+template <int HK>
 __global__ void insert_letters_kernel(const __grid_constant__ LevelArgs A, int nalpha) {
     const int lane = threadIdx.x & 31;
     const int nch = A.pitch >> 1;
@@ -619,7 +652,7 @@ __global__ void insert_letters_kernel(const __grid_constant__ LevelArgs A, int n
         u64 k = (2ull * lane + 1ull) * WEYL;
         for (int c = lane; c < nch; c += 32, k += 64ull * WEYL) {
             const ulonglong2 w = reinterpret_cast<const ulonglong2 *>(row)[c];
-            h[0] += hw(w.x, k, 2 * c < A.n) + hw(w.y, k + WEYL, 2 * c + 1 < A.n);
+            h[0] += hw<HK>(w.x, k, 2 * c < A.n) + hw<HK>(w.y, k + WEYL, 2 * c + 1 < A.n);
         }
         (void)meta;
         const u64 sum = reduce_to_lane<1>(h, lane);
@@ -668,7 +701,7 @@ __global__ void insert_letters_kernel(const __grid_constant__ LevelArgs A, int n
                     bool diff = false;
                     const ulonglong2 *ex = reinterpret_cast<const ulonglong2 *>(A.cache + other * A.pitch);
                     for (int c = lane; c < nch; c += 32) {
-                        const ulonglong2 a = g.word2(0, c), b = __ldcg(ex + c);
+                        const ulonglong2 a = g.word(0, c, g.pre(c)), b = __ldcg(ex + c);
                         diff |= (a.x != b.x) | (a.y != b.y);
                     }
                     same = !__any_sync(FULL, diff);
@@ -743,8 +776,8 @@ __global__ void apply_op_kernel(int op, const u64 *a, const u64 *b, const u64 *w
         out[(u64)row * pitch + i] = w;
         if (out2) out2[(u64)row * pitch + i] = w2;
         const u64 key = (u64)(i + 1) * WEYL;
-        h1 += hw(w, key, i < n);
-        h2 += hw(w2, key, i < n);
+        h1 += hw<1>(w, key, i < n);
+        h2 += hw<1>(w2, key, i < n);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -761,45 +794,49 @@ __global__ void apply_op_kernel(int op, const u64 *a, const u64 *b, const u64 *w
 
 int level_kernel_smem_bytes(int left_tile, int pitch) { return left_tile * pitch * 8; }
 
-int level_kernel_max_ctas_per_sm(int left_tile, int block, int smem) {
+template <int TL, int HK>
+static int occupancy_tl(int block, int smem) {
     int n = 0;
-    cudaError_t e;
-    if (left_tile == 4)
-        cudaFuncSetAttribute(level_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    else if (left_tile == 16)
-        cudaFuncSetAttribute(level_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    else
-        cudaFuncSetAttribute(level_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (left_tile == 4)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<4>, block, smem);
-    else if (left_tile == 16)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<16>, block, smem);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<8>, block, smem);
-    return e == cudaSuccess ? n : 0;
+    cudaFuncSetAttribute(level_kernel<TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<TL, HK>, block, smem) == cudaSuccess ? n
+                                                                                                            : 0;
 }
 
-template <int TL>
+int level_kernel_max_ctas_per_sm(int left_tile, int block, int smem) {
+    if (left_tile == 4) return occupancy_tl<4, 0>(block, smem);
+    if (left_tile == 16) return occupancy_tl<16, 0>(block, smem);
+    return occupancy_tl<8, 0>(block, smem);
+}
+
+template <int TL, int HK>
 static cudaError_t launch_tl(const LevelArgs &a, int grid, int block, cudaStream_t s) {
     const int smem = level_kernel_smem_bytes(TL, a.pitch);
     static int attr_set = -1;  // largest dynamic shared memory size enabled so far
     if (smem > 48 * 1024 && smem > attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(level_kernel<TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaError_t e = cudaFuncSetAttribute(level_kernel<TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         attr_set = smem;
     }
-    level_kernel<TL><<<grid, block, smem, s>>>(a);
+    level_kernel<TL, HK><<<grid, block, smem, s>>>(a);
     return cudaGetLastError();
 }
 
+template <int HK>
+static cudaError_t launch_hk(const LevelArgs &a, int grid, int block, cudaStream_t s) {
+    if (a.left_tile == 4) return launch_tl<4, HK>(a, grid, block, s);
+    if (a.left_tile == 16) return launch_tl<16, HK>(a, grid, block, s);
+    return launch_tl<8, HK>(a, grid, block, s);
+}
+
 cudaError_t launch_level(const LevelArgs &a, int grid, int block, cudaStream_t s) {
-    if (a.left_tile == 4) return launch_tl<4>(a, grid, block, s);
-    if (a.left_tile == 16) return launch_tl<16>(a, grid, block, s);
-    return launch_tl<8>(a, grid, block, s);
+    return a.key_mode == KEY_HASH64 ? launch_hk<1>(a, grid, block, s) : launch_hk<0>(a, grid, block, s);
 }
 
 cudaError_t launch_insert_letters(const LevelArgs &a, int nalpha, cudaStream_t s) {
-    insert_letters_kernel<<<1, 32, 0, s>>>(a, nalpha);
+    if (a.key_mode == KEY_HASH64)
+        insert_letters_kernel<1><<<1, 32, 0, s>>>(a, nalpha);
+    else
+        insert_letters_kernel<0><<<1, 32, 0, s>>>(a, nalpha);
     return cudaGetLastError();
 }
 

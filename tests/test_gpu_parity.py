@@ -170,3 +170,36 @@ def test_engine_reuse_many_instances(engine):
         ref = O.learn(inst, neg_type=1)
         assert res.cost == ref.cost, seed
         assert O.separates(res.formula, inst)
+
+
+def _golden_exact_runs():
+    from helpers import reference_runs
+    runs = reference_runs()
+    if not runs:
+        return []
+    out = []
+    for r in runs["runs"]:
+        inst = load_fixture(r["file"])
+        if r["final"]["limits_error"] or lensum(inst) > 126:
+            continue
+        out.append(r)
+    return out
+
+
+@pytest.mark.parametrize("run", _golden_exact_runs(), ids=lambda r: r["id"])
+def test_gpu_matches_reference_outputs(engine, run):
+    """Per-block schedule vs the reference binary's own progress lines (exact regime)."""
+    inst = load_fixture(run["file"])
+    res = engine.learn(inst, costs=run["costs"], max_cost=run["max_cost"], neg_type=run["neg"],
+                       schedule=api.SCHEDULE_PER_BLOCK, limit_traces=True)
+    mine = [[b["cost"], b["op"], b["all_before"], b["stored_before"], b["to_check"]] for b in res.blocks]
+    ref = [p for p in run["progress"] if p[1] != "A"]
+    assert mine == ref
+    fin = run["final"]
+    assert res.cost == fin["cost"] and res.all_ltls == fin["all_ltls"]
+    if fin["formula"] == "not_found":
+        assert res.status == api.NOT_FOUND and res.formula == "not_found"
+    else:
+        assert res.status == api.FOUND
+        assert O.separates(res.formula, inst)
+        assert O.formula_cost(res.formula, run["costs"]) == fin["cost"]

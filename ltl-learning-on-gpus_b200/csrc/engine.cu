@@ -63,6 +63,8 @@ struct ltlg_engine {
     ltlg_engine_config cfg{};
     int num_sms = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t op_stream[7] = {};   // one per operator kernel, forked from and joined to stream
+    cudaEvent_t ev_fork = nullptr, ev_join[7] = {};
     cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
     DevBuf cache, parents, keys, slots, wmeta, kmeta, ctl, blocks, walk, snaps;
     DevBuf h_ctl, h_blocks, h_walk, h_stage, h_snaps;
@@ -219,7 +221,7 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
         ltlg_default_engine_config(&cfg);
     if (cfg.device < 0 || cfg.device >= ndev) return LTLG_BAD_ARGS;
     if (cfg.slots_log2 < 10 || cfg.slots_log2 > 34) return LTLG_BAD_ARGS;
-    if (cfg.left_tile != 4 && cfg.left_tile != 8 && cfg.left_tile != 16) return LTLG_BAD_ARGS;
+    if (cfg.left_tile != 4 && cfg.left_tile != 8) return LTLG_BAD_ARGS;
     if (cfg.block_threads < 32 || cfg.block_threads > 256 || cfg.block_threads % 32) return LTLG_BAD_ARGS;
     if (cfg.right_chunk < 1 || cfg.unary_rows < 1 || cfg.max_traces < 1) return LTLG_BAD_ARGS;
     if (cfg.max_rows <= 0 || cfg.max_rows > (1ll << 30) - 1) cfg.max_rows = (1ll << 30) - 1;
@@ -228,6 +230,11 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
     cudaError_t err = cudaSetDevice(cfg.device);
     if (err == cudaSuccess) err = cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, cfg.device);
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    for (int k = 0; k < 7 && err == cudaSuccess; ++k) {
+        err = cudaStreamCreateWithFlags(&e->op_stream[k], cudaStreamNonBlocking);
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_join[k], cudaEventDisableTiming);
+    }
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming);
     if (err == cudaSuccess) err = cudaEventCreate(&e->ev_a);
     if (err == cudaSuccess) err = cudaEventCreate(&e->ev_b);
     if (err == cudaSuccess) err = cudaEventCreate(&e->ev_t0);
@@ -258,8 +265,12 @@ LTLG_API void ltlg_engine_destroy(ltlg_engine *e) {
         if (b->p) cudaFree(b->p);
     for (DevBuf *b : {&e->h_ctl, &e->h_blocks, &e->h_walk, &e->h_stage, &e->h_snaps})
         if (b->p) cudaFreeHost(b->p);
-    for (cudaEvent_t ev : {e->ev_a, e->ev_b, e->ev_t0, e->ev_t1})
+    for (cudaEvent_t ev : {e->ev_a, e->ev_b, e->ev_t0, e->ev_t1, e->ev_fork})
         if (ev) cudaEventDestroy(ev);
+    for (int k = 0; k < 7; ++k) {
+        if (e->ev_join[k]) cudaEventDestroy(e->ev_join[k]);
+        if (e->op_stream[k]) cudaStreamDestroy(e->op_stream[k]);
+    }
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -447,8 +458,8 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     A.right_chunk = e->cfg.right_chunk;
     A.unary_rows = e->cfg.unary_rows;
     int tl = e->cfg.left_tile;
-    while (tl > 4 && (size_t)level_kernel_smem_bytes(tl, pitch) > 200 * 1024) tl /= 2;
-    if ((size_t)level_kernel_smem_bytes(tl, pitch) > 220 * 1024) {
+    while (tl > 4 && (size_t)op_kernel_smem_bytes(OP_AND, tl, pitch) > 200 * 1024) tl /= 2;
+    if ((size_t)op_kernel_smem_bytes(OP_AND, tl, pitch) > 220 * 1024) {
         res->status = LTLG_BAD_ARGS;
         res->formula = strdup("bad_arguments");
         return res->status;
@@ -458,10 +469,14 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     int launches = 1;
 
     const int block_threads = e->cfg.block_threads;
-    const int smem = level_kernel_smem_bytes(tl, pitch);
-    int per_sm = level_kernel_max_ctas_per_sm(tl, block_threads, smem);
-    if (per_sm < 1) per_sm = 1;
-    const long long max_grid = (long long)e->num_sms * per_sm;
+    long long max_grid_op[7];
+    long long max_grid = 0;
+    for (int k = 0; k < 7; ++k) {
+        const int per_sm = std::max(1, op_kernel_max_ctas_per_sm(k, tl, A.key_mode == KEY_HASH64 ? 1 : 0,
+                                                                 block_threads, pitch));
+        max_grid_op[k] = (long long)e->num_sms * per_sm;
+        max_grid = std::max(max_grid, max_grid_op[k]);
+    }
 
     std::vector<ltlg_level_stat> lstats;
     std::vector<ltlg_block_stat> bstats;
@@ -518,8 +533,9 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
             d.r1 = B.r1;
             d.item0 = items;
             if (B.op == OP_AND || B.op == OP_OR || B.op == OP_U) {
+                const int tile = B.op == OP_U ? tl / 2 : tl;  // U: two candidates per pair
                 d.tiles_r = (B.r1 - B.r0 + A.right_chunk - 1) / A.right_chunk;
-                d.items = ((B.l1 - B.l0 + tl - 1) / tl) * d.tiles_r;
+                d.items = ((B.l1 - B.l0 + tile - 1) / tile) * d.tiles_r;
             } else {
                 d.tiles_r = 1;
                 d.items = (B.r1 - B.r0 + A.unary_rows - 1) / A.unary_rows;
@@ -528,31 +544,56 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
             hb[b] = d;
         }
         const long long stored_before = ls[cost];
+        // Items are numbered per operator (each operator's kernel drains its own queue);
+        // the per-block schedule numbers every block from 0.
+        {
+            long long op_items[7] = {0, 0, 0, 0, 0, 0, 0};
+            for (size_t b = 0; b < nb; ++b) {
+                const int op = hb[b].op;
+                hb[b].item0 = per_block ? 0 : op_items[op];
+                op_items[op] += hb[b].items;
+            }
+        }
         if (nb) cudaMemcpyAsync(e->blocks.p, hb, nb * sizeof(BlockDesc), cudaMemcpyHostToDevice, st);
-        A.blocks = (const BlockDesc *)e->blocks.p;
         A.check_only = on_the_fly ? 1 : 0;
-        if (!per_block && items > 0) cudaMemsetAsync(&((DevCtl *)e->ctl.p)->queue_head, 0, sizeof(u64), st);
+        DevCtl *dctl = (DevCtl *)e->ctl.p;
+        if (!per_block && items > 0) cudaMemsetAsync(dctl->queue, 0, sizeof(dctl->queue), st);
         cudaEventRecord(e->ev_a, st);
         if (!per_block) {
             if (items > 0) {
-                A.nblocks = (int)nb;
-                A.total_items = items;
-                const int grid = (int)std::min<long long>(items, max_grid);
-                if ((err = launch_level(A, grid, block_threads, st)) != cudaSuccess) return fail_cuda(e, err, res);
-                ++launches;
+                // fork: every operator with work runs concurrently on its own stream
+                cudaEventRecord(e->ev_fork, st);
+                size_t b = 0;
+                while (b < nb) {
+                    const int op = hb[b].op;
+                    size_t b2 = b;
+                    long long op_total = 0;
+                    while (b2 < nb && hb[b2].op == op) op_total += hb[b2++].items;
+                    A.blocks = (const BlockDesc *)e->blocks.p + b;
+                    A.nblocks = (int)(b2 - b);
+                    A.total_items = op_total;
+                    A.queue = dctl->queue + op;
+                    cudaStreamWaitEvent(e->op_stream[op], e->ev_fork, 0);
+                    const int grid = (int)std::min<long long>(op_total, max_grid_op[op]);
+                    if ((err = launch_op(op, A, grid, block_threads, e->op_stream[op])) != cudaSuccess)
+                        return fail_cuda(e, err, res);
+                    ++launches;
+                    cudaEventRecord(e->ev_join[op], e->op_stream[op]);
+                    cudaStreamWaitEvent(st, e->ev_join[op], 0);
+                    b = b2;
+                }
             }
         } else {
             for (size_t b = 0; b < nb; ++b) {
+                const int op = hb[b].op;
                 cudaMemcpyAsync((DevCtl *)e->snaps.p + b, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToDevice, st);
-                const u64 start = (u64)hb[b].item0;
-                cudaMemcpyAsync(&((DevCtl *)e->ctl.p)->queue_head, &hb[b].item0, sizeof(u64), cudaMemcpyHostToDevice,
-                                st);
-                (void)start;
+                cudaMemsetAsync(dctl->queue + op, 0, sizeof(u64), st);
                 A.blocks = (const BlockDesc *)e->blocks.p + b;
                 A.nblocks = 1;
-                A.total_items = hb[b].item0 + hb[b].items;
-                const int grid = (int)std::min<long long>(hb[b].items, max_grid);
-                if ((err = launch_level(A, grid, block_threads, st)) != cudaSuccess) return fail_cuda(e, err, res);
+                A.total_items = hb[b].items;
+                A.queue = dctl->queue + op;
+                const int grid = (int)std::min<long long>(hb[b].items, max_grid_op[op]);
+                if ((err = launch_op(op, A, grid, block_threads, st)) != cudaSuccess) return fail_cuda(e, err, res);
                 ++launches;
             }
         }

@@ -180,7 +180,7 @@ struct BinGen {
     const ulonglong2 *left;   // shared-memory tile, row stride nch
     const ulonglong2 *right;  // global right row
     int nch;
-    __device__ __forceinline__ ulonglong2 pre(int c) const { return right[c]; }
+    __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldg(right + c); }
     __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 r) const {
         if (OP == OP_U) {
             const ulonglong2 l = left[(t >> 1) * nch + c];
@@ -200,7 +200,7 @@ struct UnGen {
     int pitch;
     __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldg(meta + c); }
     __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 m) const {
-        const ulonglong2 s = reinterpret_cast<const ulonglong2 *>(src0 + (size_t)t * pitch)[c];
+        const ulonglong2 s = __ldg(reinterpret_cast<const ulonglong2 *>(src0 + (size_t)t * pitch) + c);
         return make_ulonglong2(uop<OP>(s.x, m.x), uop<OP>(s.y, m.y));
     }
 };
@@ -481,17 +481,33 @@ __device__ void unary_item(const LevelArgs &A, const BlockDesc &B, long long loc
 #pragma unroll
         for (int t = 0; t < UNARY_GROUP; ++t) h[t] = 0;
         u32 bad = 0;
-        u64 k = (2ull * lane + 1ull) * WEYL;
-        for (int c = lane; c < nch; c += 32, k += 64ull * WEYL) {
-            const ulonglong2 m = __ldg(meta + c);
-            const bool v0 = 2 * c < A.n, v1 = 2 * c + 1 < A.n;
+        for (int c0 = lane; c0 < nch; c0 += 64) {
+            ulonglong2 sv[2][UNARY_GROUP], mv[2];
 #pragma unroll
-            for (int t = 0; t < UNARY_GROUP; ++t) {
-                if (t < cnt) {
-                    const ulonglong2 sv = reinterpret_cast<const ulonglong2 *>(src0 + (size_t)t * A.pitch)[c];
-                    const u64 w0 = uop<OP>(sv.x, m.x), w1 = uop<OP>(sv.y, m.y);
-                    h[t] += hw<HK>(w0, k, v0) + hw<HK>(w1, k + WEYL, v1);
-                    bad |= badbit(w0, w1, m.x, m.y) << t;
+            for (int u = 0; u < 2; ++u) {
+                const int c = c0 + 32 * u;
+                if (c < nch) {
+                    mv[u] = __ldg(meta + c);
+#pragma unroll
+                    for (int t = 0; t < UNARY_GROUP; ++t)
+                        if (t < cnt) sv[u][t] = __ldg(reinterpret_cast<const ulonglong2 *>(src0 + (size_t)t * A.pitch) + c);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int c = c0 + 32 * u;
+                if (c < nch) {
+                    const u64 k = (2ull * (u64)c + 1ull) * WEYL;
+                    const bool v0 = 2 * c < A.n, v1 = 2 * c + 1 < A.n;
+                    const ulonglong2 m = mv[u];
+#pragma unroll
+                    for (int t = 0; t < UNARY_GROUP; ++t) {
+                        if (t < cnt) {
+                            const u64 w0 = uop<OP>(sv[u][t].x, m.x), w1 = uop<OP>(sv[u][t].y, m.y);
+                            h[t] += hw<HK>(w0, k, v0) + hw<HK>(w1, k + WEYL, v1);
+                            bad |= badbit(w0, w1, m.x, m.y) << t;
+                        }
+                    }
                 }
             }
         }
@@ -512,29 +528,41 @@ __device__ void binary_row(const LevelArgs &A, const ulonglong2 *tile, int nl, l
 #pragma unroll
     for (int t = 0; t < NC; ++t) h[t] = 0;
     u32 bad = 0;
-    u64 k = (2ull * lane + 1ull) * WEYL;
-#pragma unroll 2
-    for (int c = lane; c < nch; c += 32, k += 64ull * WEYL) {
-        const ulonglong2 rv = R[c];
-        const ulonglong2 m = __ldg(meta + c);
-        const bool v0 = 2 * c < A.n, v1 = 2 * c + 1 < A.n;
-        const u64 rx = OP == OP_U ? rev62(rv.x) : 0ull, ry = OP == OP_U ? rev62(rv.y) : 0ull;
+    for (int c0 = lane; c0 < nch; c0 += 128) {
+        ulonglong2 rvv[4], mv[4];
 #pragma unroll
-        for (int t = 0; t < TL; ++t) {
-            if (t < nl) {
-                const ulonglong2 lv = tile[t * nch + c];
-                if (OP == OP_U) {
-                    const u64 lx = rev62(lv.x), ly = rev62(lv.y);
-                    const u64 ax = lx | rx, ay = ly | ry;
-                    const u64 a0 = until_rev(ax, rx), a1 = until_rev(ay, ry);  // l U r
-                    const u64 b0 = until_rev(ax, lx), b1 = until_rev(ay, ly);  // r U l
-                    h[2 * t] += hw<HK>(a0, k, v0) + hw<HK>(a1, k + WEYL, v1);
-                    h[2 * t + 1] += hw<HK>(b0, k, v0) + hw<HK>(b1, k + WEYL, v1);
-                    bad |= (badbit(a0, a1, m.x, m.y) << (2 * t)) | (badbit(b0, b1, m.x, m.y) << (2 * t + 1));
-                } else {
-                    const u64 w0 = bop<OP>(lv.x, rv.x), w1 = bop<OP>(lv.y, rv.y);
-                    h[t] += hw<HK>(w0, k, v0) + hw<HK>(w1, k + WEYL, v1);
-                    bad |= badbit(w0, w1, m.x, m.y) << t;
+        for (int u = 0; u < 4; ++u) {
+            const int c = c0 + 32 * u;
+            if (c < nch) {
+                rvv[u] = __ldg(R + c);
+                mv[u] = __ldg(meta + c);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int c = c0 + 32 * u;
+            if (c >= nch) continue;
+            const u64 k = (2ull * (u64)c + 1ull) * WEYL;
+            const ulonglong2 rv = rvv[u], m = mv[u];
+            const bool v0 = 2 * c < A.n, v1 = 2 * c + 1 < A.n;
+            const u64 rx = OP == OP_U ? rev62(rv.x) : 0ull, ry = OP == OP_U ? rev62(rv.y) : 0ull;
+#pragma unroll
+            for (int t = 0; t < TL; ++t) {
+                if (t < nl) {
+                    const ulonglong2 lv = tile[t * nch + c];
+                    if (OP == OP_U) {
+                        const u64 lx = rev62(lv.x), ly = rev62(lv.y);
+                        const u64 ax = lx | rx, ay = ly | ry;
+                        const u64 a0 = until_rev(ax, rx), a1 = until_rev(ay, ry);  // l U r
+                        const u64 b0 = until_rev(ax, lx), b1 = until_rev(ay, ly);  // r U l
+                        h[2 * t] += hw<HK>(a0, k, v0) + hw<HK>(a1, k + WEYL, v1);
+                        h[2 * t + 1] += hw<HK>(b0, k, v0) + hw<HK>(b1, k + WEYL, v1);
+                        bad |= (badbit(a0, a1, m.x, m.y) << (2 * t)) | (badbit(b0, b1, m.x, m.y) << (2 * t + 1));
+                    } else {
+                        const u64 w0 = bop<OP>(lv.x, rv.x), w1 = bop<OP>(lv.y, rv.y);
+                        h[t] += hw<HK>(w0, k, v0) + hw<HK>(w1, k + WEYL, v1);
+                        bad |= badbit(w0, w1, m.x, m.y) << t;
+                    }
                 }
             }
         }
@@ -556,9 +584,10 @@ __device__ void binary_row(const LevelArgs &A, const ulonglong2 *tile, int nl, l
 template <int OP, int TL, int HK>
 __device__ bool binary_item(const LevelArgs &A, const BlockDesc &B, long long local, u64 *tile, u64 *bar,
                             u32 &phase, int warp, int nwarps, int lane, u64 &evals) {
+    constexpr int TLOP = OP == OP_U ? TL / 2 : TL;  // U makes two candidates per pair
     const long long tl = local / B.tiles_r, tr = local % B.tiles_r;
-    const long long l_first = B.l0 + tl * TL;
-    const int nl = (int)min((long long)TL, B.l1 - l_first);
+    const long long l_first = B.l0 + tl * TLOP;
+    const int nl = (int)min((long long)TLOP, B.l1 - l_first);
     const long long r_first = B.r0 + tr * A.right_chunk;
     const long long r_end = min(B.r1, r_first + (long long)A.right_chunk);
     if (threadIdx.x == 0) {
@@ -577,13 +606,17 @@ __device__ bool binary_item(const LevelArgs &A, const BlockDesc &B, long long lo
     const ulonglong2 *t2 = reinterpret_cast<const ulonglong2 *>(tile);
     for (long long r = r_first + warp; r < r_end; r += nwarps) {
         if (__any_sync(FULL, found_stop(A))) break;  // warp-uniform: lanes must not split
-        binary_row<OP, TL, HK>(A, t2, nl, l_first, r, lane, evals);
+        binary_row<OP, TLOP, HK>(A, t2, nl, l_first, r, lane, evals);
     }
     return true;
 }
 
-template <int TL, int HK>
-__global__ void __launch_bounds__(256, 3) level_kernel(const __grid_constant__ LevelArgs A) {
+// One operator's work items.  Binary kernels stage a left tile per item with a bulk
+// copy; unary kernels use no shared memory.
+template <int OP, int TL, int HK>
+__global__ void __launch_bounds__(256, (OP == OP_AND || OP == OP_OR || OP == OP_U) ? 3 : 4)
+    op_kernel(const __grid_constant__ LevelArgs A) {
+    constexpr bool BIN = OP == OP_AND || OP == OP_OR || OP == OP_U;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     u64 *tile = reinterpret_cast<u64 *>(smem_raw);
     __shared__ __align__(8) u64 bar;
@@ -591,8 +624,10 @@ __global__ void __launch_bounds__(256, 3) level_kernel(const __grid_constant__ L
     __shared__ u64 s_evals;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     if (threadIdx.x == 0) {
-        mbar_init(&bar, 1);
-        fence_mbar_init();
+        if (BIN) {
+            mbar_init(&bar, 1);
+            fence_mbar_init();
+        }
         s_evals = 0;
     }
     __syncthreads();
@@ -602,7 +637,7 @@ __global__ void __launch_bounds__(256, 3) level_kernel(const __grid_constant__ L
         if (threadIdx.x == 0) {
             long long it = -1;
             if (!found_stop(A)) {
-                it = (long long)atomicAdd(&A.ctl->queue_head, 1ull);
+                it = (long long)atomicAdd(A.queue, 1ull);
                 if (it >= A.total_items) it = -1;
             }
             s_item = it;
@@ -620,18 +655,11 @@ __global__ void __launch_bounds__(256, 3) level_kernel(const __grid_constant__ L
         }
         const BlockDesc B = A.blocks[lo];
         const long long local = item - B.item0;
-        bool ok = true;
-        switch (B.op) {
-        case OP_NEG: unary_item<OP_NEG, HK>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_X: unary_item<OP_X, HK>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_F: unary_item<OP_F, HK>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_G: unary_item<OP_G, HK>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_AND: ok = binary_item<OP_AND, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
-        case OP_OR: ok = binary_item<OP_OR, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
-        case OP_U: ok = binary_item<OP_U, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
-        default: break;
+        if (BIN) {
+            if (!binary_item<OP, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals)) break;
+        } else {
+            unary_item<OP, HK>(A, B, local, warp, nwarps, lane, evals);
         }
-        if (!ok) break;
         __syncthreads();
     }
     if (lane == 0 && evals) atomicAdd(&s_evals, evals);
@@ -792,44 +820,75 @@ __global__ void apply_op_kernel(int op, const u64 *a, const u64 *b, const u64 *w
 
 }  // namespace
 
-int level_kernel_smem_bytes(int left_tile, int pitch) { return left_tile * pitch * 8; }
-
-template <int TL, int HK>
-static int occupancy_tl(int block, int smem) {
-    int n = 0;
-    cudaFuncSetAttribute(level_kernel<TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<TL, HK>, block, smem) == cudaSuccess ? n
-                                                                                                            : 0;
+int op_kernel_smem_bytes(int op, int left_tile, int pitch) {
+    if (op == OP_AND || op == OP_OR) return left_tile * pitch * 8;
+    if (op == OP_U) return (left_tile / 2) * pitch * 8;
+    return 0;
 }
 
-int level_kernel_max_ctas_per_sm(int left_tile, int block, int smem) {
-    if (left_tile == 4) return occupancy_tl<4, 0>(block, smem);
-    if (left_tile == 16) return occupancy_tl<16, 0>(block, smem);
-    return occupancy_tl<8, 0>(block, smem);
-}
-
-template <int TL, int HK>
-static cudaError_t launch_tl(const LevelArgs &a, int grid, int block, cudaStream_t s) {
-    const int smem = level_kernel_smem_bytes(TL, a.pitch);
+template <int OP, int TL, int HK>
+static cudaError_t launch_one(const LevelArgs &a, int grid, int block, cudaStream_t s) {
+    const int smem = op_kernel_smem_bytes(OP, TL, a.pitch);
     static int attr_set = -1;  // largest dynamic shared memory size enabled so far
     if (smem > 48 * 1024 && smem > attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(level_kernel<TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaError_t e = cudaFuncSetAttribute(op_kernel<OP, TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         attr_set = smem;
     }
-    level_kernel<TL, HK><<<grid, block, smem, s>>>(a);
+    op_kernel<OP, TL, HK><<<grid, block, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-template <int HK>
-static cudaError_t launch_hk(const LevelArgs &a, int grid, int block, cudaStream_t s) {
-    if (a.left_tile == 4) return launch_tl<4, HK>(a, grid, block, s);
-    if (a.left_tile == 16) return launch_tl<16, HK>(a, grid, block, s);
-    return launch_tl<8, HK>(a, grid, block, s);
+template <int OP, int TL, int HK>
+static int occupancy_one(int block, int pitch) {
+    const int smem = op_kernel_smem_bytes(OP, TL, pitch);
+    int n = 0;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(op_kernel<OP, TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, op_kernel<OP, TL, HK>, block, smem) == cudaSuccess ? n
+                                                                                                                : 0;
 }
 
-cudaError_t launch_level(const LevelArgs &a, int grid, int block, cudaStream_t s) {
-    return a.key_mode == KEY_HASH64 ? launch_hk<1>(a, grid, block, s) : launch_hk<0>(a, grid, block, s);
+template <int TL, int HK>
+static cudaError_t launch_tl(int op, const LevelArgs &a, int grid, int block, cudaStream_t s) {
+    switch (op) {
+    case OP_NEG: return launch_one<OP_NEG, TL, HK>(a, grid, block, s);
+    case OP_AND: return launch_one<OP_AND, TL, HK>(a, grid, block, s);
+    case OP_OR: return launch_one<OP_OR, TL, HK>(a, grid, block, s);
+    case OP_X: return launch_one<OP_X, TL, HK>(a, grid, block, s);
+    case OP_F: return launch_one<OP_F, TL, HK>(a, grid, block, s);
+    case OP_G: return launch_one<OP_G, TL, HK>(a, grid, block, s);
+    case OP_U: return launch_one<OP_U, TL, HK>(a, grid, block, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int TL, int HK>
+static int occupancy_tl(int op, int block, int pitch) {
+    switch (op) {
+    case OP_NEG: return occupancy_one<OP_NEG, TL, HK>(block, pitch);
+    case OP_AND: return occupancy_one<OP_AND, TL, HK>(block, pitch);
+    case OP_OR: return occupancy_one<OP_OR, TL, HK>(block, pitch);
+    case OP_X: return occupancy_one<OP_X, TL, HK>(block, pitch);
+    case OP_F: return occupancy_one<OP_F, TL, HK>(block, pitch);
+    case OP_G: return occupancy_one<OP_G, TL, HK>(block, pitch);
+    case OP_U: return occupancy_one<OP_U, TL, HK>(block, pitch);
+    default: return 0;
+    }
+}
+
+cudaError_t launch_op(int op, const LevelArgs &a, int grid, int block, cudaStream_t s) {
+    if (a.key_mode == KEY_HASH64) {
+        if (a.left_tile == 4) return launch_tl<4, 1>(op, a, grid, block, s);
+        return launch_tl<8, 1>(op, a, grid, block, s);
+    }
+    if (a.left_tile == 4) return launch_tl<4, 0>(op, a, grid, block, s);
+    return launch_tl<8, 0>(op, a, grid, block, s);
+}
+
+int op_kernel_max_ctas_per_sm(int op, int left_tile, int hash_kind, int block, int pitch) {
+    if (hash_kind == 1) return left_tile == 4 ? occupancy_tl<4, 1>(op, block, pitch) : occupancy_tl<8, 1>(op, block, pitch);
+    return left_tile == 4 ? occupancy_tl<4, 0>(op, block, pitch) : occupancy_tl<8, 0>(op, block, pitch);
 }
 
 cudaError_t launch_insert_letters(const LevelArgs &a, int nalpha, cudaStream_t s) {

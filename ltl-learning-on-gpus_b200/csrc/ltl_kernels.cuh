@@ -33,9 +33,9 @@ struct DevCtl {
     u64 row_count;   // rows handed out, letters included (may pass cap_rows on overflow)
     u64 found;       // 0, or (1 << 63) | parents of an accepting candidate
     u64 evaluated;   // candidates evaluated
-    u64 queue_head;  // next work item of the current launch
     u32 status;      // ST_* bits
     u32 pad;
+    u64 queue[8];    // next work item of each operator's kernel
 };
 
 // One (operator, split) block of a level.  Unary: source rows [r0, r1).
@@ -50,7 +50,8 @@ struct BlockDesc {
 };
 
 struct LevelArgs {
-    const BlockDesc *blocks;
+    const BlockDesc *blocks;  // this operator's blocks
+    u64 *queue;               // this operator's work-item counter
     int nblocks;
     int n;               // traces = words per CS
     int pitch;           // words per cache row (n rounded up to a multiple of 4)
@@ -75,10 +76,11 @@ struct LevelArgs {
     int left_tile;
 };
 
-// Launch wrappers (ltl_kernels.cu).
-int level_kernel_smem_bytes(int left_tile, int pitch);
-cudaError_t launch_level(const LevelArgs &a, int grid, int block, cudaStream_t s);
-int level_kernel_max_ctas_per_sm(int left_tile, int block, int smem);
+// Launch wrappers (ltl_kernels.cu).  One kernel per operator drains the work items of
+// that operator's blocks; binary kernels stage left tiles of left_tile rows (U: half).
+int op_kernel_smem_bytes(int op, int left_tile, int pitch);
+cudaError_t launch_op(int op, const LevelArgs &a, int grid, int block, cudaStream_t s);
+int op_kernel_max_ctas_per_sm(int op, int left_tile, int hash_kind, int block, int pitch);
 cudaError_t launch_insert_letters(const LevelArgs &a, int nalpha, cudaStream_t s);
 cudaError_t launch_walk(const u64 *parents, int nalpha, u64 found, u64 *out, int cap, cudaStream_t s);
 cudaError_t launch_apply_op(int op, const u64 *a, const u64 *b, const u64 *wmeta, int n, int pitch, int count,

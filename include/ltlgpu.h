@@ -164,6 +164,19 @@ LTLG_API int ltlg_learn(const ltlg_traces *traces, const ltlg_options *opt, ltlg
 
 LTLG_API void ltlg_result_free(ltlg_result *res);
 
+/* Batched learning: independent instances spread over `workers` engines (each with its own
+ * stream and device buffers, driven by its own host thread), so the latency-bound small
+ * levels of different instances overlap on the GPU.  results[i] belongs to traces[i];
+ * free each with ltlg_result_free.  The reference has one instance per process
+ * (code/dc.py:33-43 runs the binary once per sub-problem); this replaces that loop. */
+typedef struct ltlg_batch ltlg_batch;
+LTLG_API int ltlg_batch_create(const ltlg_engine_config *cfg, int32_t workers, ltlg_batch **out);
+LTLG_API void ltlg_batch_destroy(ltlg_batch *b);
+LTLG_API int ltlg_batch_learn(ltlg_batch *b, const ltlg_traces *traces, int32_t count, const ltlg_options *opt,
+                              ltlg_result *results);
+/* Stream of worker w's engine (for event timing around batch calls). */
+LTLG_API void *ltlg_batch_stream(ltlg_batch *b, int32_t worker);
+
 /* After a learn: copy cache rows [first, first + count) (n words each, pitch dropped) and
  * their packed parents (op << 60 | left << 30 | right) to host memory.  Either pointer may
  * be NULL.  Returns 0 or an ltlg_status. */

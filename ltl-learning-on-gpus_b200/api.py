@@ -28,7 +28,8 @@ EXPORTED = [
     "ltlg_abi_version", "ltlg_status_string", "ltlg_default_engine_config", "ltlg_default_options",
     "ltlg_engine_create", "ltlg_engine_destroy", "ltlg_engine_learn", "ltlg_learn", "ltlg_result_free",
     "ltlg_engine_read_rows", "ltlg_engine_level_starts", "ltlg_device_apply_op", "ltlg_read_scarlet",
-    "ltlg_traces_free", "ltlg_engine_stream",
+    "ltlg_traces_free", "ltlg_engine_stream", "ltlg_batch_create", "ltlg_batch_destroy", "ltlg_batch_learn",
+    "ltlg_batch_stream",
 ]
 
 
@@ -97,6 +98,12 @@ def lib():
         L.ltlg_traces_free.argtypes = [C.POINTER(Traces)]
         L.ltlg_engine_stream.argtypes = [C.c_void_p]
         L.ltlg_engine_stream.restype = C.c_void_p
+        L.ltlg_batch_create.argtypes = [C.POINTER(EngineConfig), C.c_int32, C.POINTER(C.c_void_p)]
+        L.ltlg_batch_destroy.argtypes = [C.c_void_p]
+        L.ltlg_batch_learn.argtypes = [C.c_void_p, C.POINTER(Traces), C.c_int32, C.POINTER(Options),
+                                       C.POINTER(Result)]
+        L.ltlg_batch_stream.argtypes = [C.c_void_p, C.c_int32]
+        L.ltlg_batch_stream.restype = C.c_void_p
         _lib = L
     return _lib
 
@@ -236,6 +243,68 @@ class Engine:
         if rc != 0:
             raise RuntimeError(f"read_rows failed: {status_string(rc)}")
         return rows, par
+
+
+def _engine_config(device=0, slots_log2=27, cache_bytes=16 << 30, max_rows=64 << 20, max_traces=8192,
+                   block_threads=256, left_tile=8, right_chunk=64, unary_rows=64) -> EngineConfig:
+    cfg = EngineConfig()
+    lib().ltlg_default_engine_config(C.byref(cfg))
+    cfg.device, cfg.slots_log2, cfg.cache_bytes, cfg.max_rows = device, slots_log2, cache_bytes, max_rows
+    cfg.max_traces, cfg.block_threads, cfg.left_tile = max_traces, block_threads, left_tile
+    cfg.right_chunk, cfg.unary_rows = right_chunk, unary_rows
+    return cfg
+
+
+class Batch:
+    """Independent instances learned concurrently by `workers` engines (native threads)."""
+
+    def __init__(self, workers=8, **engine_kw):
+        cfg = _engine_config(**engine_kw)
+        h = C.c_void_p()
+        rc = lib().ltlg_batch_create(C.byref(cfg), int(workers), C.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"ltlg_batch_create failed: {status_string(rc)}")
+        self._h = h
+        self.workers = workers
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ltlg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def stream(self, worker: int = 0) -> int:
+        return lib().ltlg_batch_stream(self._h, worker) or 0
+
+    def learn(self, instances, **kw) -> list:
+        o = make_options(**kw)
+        n = len(instances)
+        arr = (Traces * n)()
+        keep = []
+        for i, inst in enumerate(instances):
+            t, k = _traces(inst)
+            arr[i] = t
+            keep.append(k)
+        res = (Result * n)()
+        lib().ltlg_batch_learn(self._h, arr, n, C.byref(o), res)
+        out = []
+        for i in range(n):
+            try:
+                out.append(_result(res[i]))
+            finally:
+                lib().ltlg_result_free(C.byref(res[i]))
+        return out
 
 
 def learn(inst: Instance, **kw) -> LearnResult:

@@ -9,7 +9,9 @@
 // (or one launch per block in the per-block schedule), and the host reads a small
 // control record once per level.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <thread>
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -63,11 +65,12 @@ struct ltlg_engine {
     ltlg_engine_config cfg{};
     int num_sms = 0;
     cudaStream_t stream = nullptr;
-    cudaStream_t op_stream[7] = {};   // one per operator kernel, forked from and joined to stream
-    cudaEvent_t ev_fork = nullptr, ev_join[7] = {};
+    static constexpr int RING = 4;     // levels in flight: the host runs up to RING - 1 ahead
+    cudaEvent_t ev_start[RING] = {}, ev_kend[RING] = {}, ev_done[RING] = {};
     cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
-    DevBuf cache, parents, keys, slots, wmeta, kmeta, ctl, blocks, walk, snaps;
-    DevBuf h_ctl, h_blocks, h_walk, h_stage, h_snaps;
+    DevBuf cache, parents, keys, slots, wmeta, kmeta, ctl, walk, snaps, lev, ls, lcands;
+    DevBuf h_ctl, h_walk, h_stage, h_snaps, h_args, h_lev, h_ls, h_lcands, h_win, h_ring;
+
     u64 nslots = 0;
     u32 gen = 0;
     // last learn
@@ -230,11 +233,11 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
     cudaError_t err = cudaSetDevice(cfg.device);
     if (err == cudaSuccess) err = cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, cfg.device);
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
-    for (int k = 0; k < 7 && err == cudaSuccess; ++k) {
-        err = cudaStreamCreateWithFlags(&e->op_stream[k], cudaStreamNonBlocking);
-        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_join[k], cudaEventDisableTiming);
+    for (int k = 0; k < ltlg_engine::RING && err == cudaSuccess; ++k) {
+        err = cudaEventCreate(&e->ev_start[k]);
+        if (err == cudaSuccess) err = cudaEventCreate(&e->ev_kend[k]);
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_done[k], cudaEventDisableTiming);
     }
-    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming);
     if (err == cudaSuccess) err = cudaEventCreate(&e->ev_a);
     if (err == cudaSuccess) err = cudaEventCreate(&e->ev_b);
     if (err == cudaSuccess) err = cudaEventCreate(&e->ev_t0);
@@ -247,6 +250,18 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
     if (err == cudaSuccess) err = ensure_host(e->h_ctl, sizeof(DevCtl));
     if (err == cudaSuccess) err = ensure(e->walk, (2 + 2 * 1024) * 8);
     if (err == cudaSuccess) err = ensure_host(e->h_walk, (2 + 2 * 1024) * 8);
+    const size_t max_blocks = 7 * MAX_SPLITS;
+    if (err == cudaSuccess) err = ensure(e->snaps, max_blocks * sizeof(DevCtl));
+    if (err == cudaSuccess) err = ensure_host(e->h_snaps, max_blocks * sizeof(DevCtl));
+    if (err == cudaSuccess) err = ensure_host(e->h_win, max_blocks * 2 * sizeof(long long));
+    if (err == cudaSuccess) err = ensure_host(e->h_args, sizeof(LevelArgs));
+    if (err == cudaSuccess) err = ensure_host(e->h_ring, ltlg_engine::RING * (sizeof(DevCtl) + sizeof(DevLevel)));
+    if (err == cudaSuccess) err = ensure(e->lev, sizeof(DevLevel));
+    if (err == cudaSuccess) err = ensure_host(e->h_lev, sizeof(DevLevel));
+    if (err == cudaSuccess) err = ensure(e->ls, (MAX_COSTS + 2) * sizeof(long long));
+    if (err == cudaSuccess) err = ensure_host(e->h_ls, (MAX_COSTS + 2) * sizeof(long long));
+    if (err == cudaSuccess) err = ensure(e->lcands, (MAX_COSTS + 2) * sizeof(u64));
+    if (err == cudaSuccess) err = ensure_host(e->h_lcands, (MAX_COSTS + 2) * sizeof(u64));
     if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
     if (err != cudaSuccess) {
         ltlg_engine_destroy(e);
@@ -260,17 +275,17 @@ LTLG_API void ltlg_engine_destroy(ltlg_engine *e) {
     if (!e) return;
     cudaSetDevice(e->cfg.device);
     if (e->stream) cudaStreamSynchronize(e->stream);
-    for (DevBuf *b : {&e->cache, &e->parents, &e->keys, &e->slots, &e->wmeta, &e->kmeta, &e->ctl, &e->blocks,
-                      &e->walk, &e->snaps})
+    for (DevBuf *b : {&e->cache, &e->parents, &e->keys, &e->slots, &e->wmeta, &e->kmeta, &e->ctl, &e->walk, &e->snaps,
+                      &e->lev, &e->ls, &e->lcands})
         if (b->p) cudaFree(b->p);
-    for (DevBuf *b : {&e->h_ctl, &e->h_blocks, &e->h_walk, &e->h_stage, &e->h_snaps})
+    for (DevBuf *b : {&e->h_ctl, &e->h_walk, &e->h_stage, &e->h_snaps, &e->h_args, &e->h_lev, &e->h_ls, &e->h_lcands,
+                      &e->h_win, &e->h_ring})
         if (b->p) cudaFreeHost(b->p);
-    for (cudaEvent_t ev : {e->ev_a, e->ev_b, e->ev_t0, e->ev_t1, e->ev_fork})
+    for (cudaEvent_t ev : {e->ev_a, e->ev_b, e->ev_t0, e->ev_t1})
         if (ev) cudaEventDestroy(ev);
-    for (int k = 0; k < 7; ++k) {
-        if (e->ev_join[k]) cudaEventDestroy(e->ev_join[k]);
-        if (e->op_stream[k]) cudaStreamDestroy(e->op_stream[k]);
-    }
+    for (int k = 0; k < ltlg_engine::RING; ++k)
+        for (cudaEvent_t ev : {e->ev_start[k], e->ev_kend[k], e->ev_done[k]})
+            if (ev) cudaEventDestroy(ev);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -438,10 +453,40 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     hc->row_count = (u64)nalpha;
     cudaMemcpyAsync(e->ctl.p, hc, sizeof(DevCtl), cudaMemcpyHostToDevice, st);
 
-    LevelArgs A{};
+    int tl = e->cfg.left_tile;
+    while (tl > 4 && (size_t)level_kernel_smem_bytes(tl, pitch) > 200 * 1024) tl /= 2;
+    if ((size_t)level_kernel_smem_bytes(tl, pitch) > 220 * 1024) {
+        res->status = LTLG_BAD_ARGS;
+        res->formula = strdup("bad_arguments");
+        return res->status;
+    }
+    const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
+    const int block_threads = e->cfg.block_threads;
+    const long long max_grid =
+        (long long)e->num_sms * std::max(1, level_kernel_max_ctas_per_sm(tl, hk, block_threads, pitch));
+
+    // Arguments and plan in device memory.
+    DevLevel *dlev = (DevLevel *)e->lev.p;
+    LevelArgs *ha = (LevelArgs *)e->h_args.p;
+    memset(ha, 0, sizeof(LevelArgs));
+    LevelArgs &A = *ha;
     A.n = n;
     A.pitch = pitch;
     A.npos = npos;
+    A.nalpha = nalpha;
+    A.key_mode = opt->key_mode == LTLG_KEY_EXACT ? KEY_EXACT : opt->key_mode == LTLG_KEY_REF ? KEY_REF : KEY_HASH64;
+    A.rlx_type = rlx_type;
+    A.gen = e->gen;
+    A.stop_at_found = opt->stop_at_found ? 1 : 0;
+    A.left_tile = tl;
+    A.neg_type = opt->neg_type;
+    A.max_cost = max_cost;
+    A.nwarps = block_threads / 32;
+    for (int i = 0; i < 8; ++i) A.cf[i] = cf[i];
+    A.right_chunk_big = e->cfg.right_chunk;
+    A.unary_rows_big = e->cfg.unary_rows;
+    A.small_level = max_grid * 2048ll;
+    A.hash_kind = hk;
     A.cap_rows = cap_rows;
     A.cache = (u64 *)e->cache.p;
     A.parents = (u64 *)e->parents.p;
@@ -451,257 +496,305 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     A.wmeta = (const u64 *)e->wmeta.p;
     A.kmeta = (const u32 *)e->kmeta.p;
     A.ctl = (DevCtl *)e->ctl.p;
-    A.key_mode = opt->key_mode == LTLG_KEY_EXACT ? KEY_EXACT : opt->key_mode == LTLG_KEY_REF ? KEY_REF : KEY_HASH64;
-    A.rlx_type = rlx_type;
-    A.gen = e->gen;
-    A.stop_at_found = opt->stop_at_found ? 1 : 0;
-    A.right_chunk = e->cfg.right_chunk;
-    A.unary_rows = e->cfg.unary_rows;
-    int tl = e->cfg.left_tile;
-    while (tl > 4 && (size_t)op_kernel_smem_bytes(OP_AND, tl, pitch) > 200 * 1024) tl /= 2;
-    if ((size_t)op_kernel_smem_bytes(OP_AND, tl, pitch) > 220 * 1024) {
-        res->status = LTLG_BAD_ARGS;
-        res->formula = strdup("bad_arguments");
-        return res->status;
-    }
-    A.left_tile = tl;
+    A.lev = dlev;
+    A.ls = (long long *)e->ls.p;
+    A.level_cands = (u64 *)e->lcands.p;
+    cudaMemsetAsync(e->ls.p, 0, (MAX_COSTS + 2) * sizeof(long long), st);
+    cudaMemsetAsync(e->lcands.p, 0, (MAX_COSTS + 2) * sizeof(u64), st);
+    DevLevel *hl = (DevLevel *)e->h_lev.p;
+    memset(hl, 0, offsetof(DevLevel, blocks));
+    hl->cost = c1;  // the planner advances to c1 + 1 first
+    cudaMemcpyAsync(dlev, hl, offsetof(DevLevel, blocks), cudaMemcpyHostToDevice, st);
     if ((err = launch_insert_letters(A, nalpha, st)) != cudaSuccess) return fail_cuda(e, err, res);
     int launches = 1;
 
-    const int block_threads = e->cfg.block_threads;
-    long long max_grid_op[7];
-    long long max_grid = 0;
-    for (int k = 0; k < 7; ++k) {
-        const int per_sm = std::max(1, op_kernel_max_ctas_per_sm(k, tl, A.key_mode == KEY_HASH64 ? 1 : 0,
-                                                                 block_threads, pitch));
-        max_grid_op[k] = (long long)e->num_sms * per_sm;
-        max_grid = std::max(max_grid, max_grid_op[k]);
-    }
-
-    std::vector<ltlg_level_stat> lstats;
-    std::vector<ltlg_block_stat> bstats;
-    std::vector<long long> &ls = e->level_start;
     int status = LTLG_NOT_FOUND;
-    bool found = false, on_the_fly = false, last_round = false;
-    int shortage = -1, cost = c1, found_cost = -1;
+    bool found = letter_hit >= 0, on_the_fly = false, last_round = false;
+    int shortage = -1, found_cost = found ? c1 : -1, last_cost = c1;
     u64 found_word = 0;
     u32 dflags = 0;
     double device_ms = 0;
+    std::vector<ltlg_block_stat> bstats;
     const bool per_block = opt->schedule == LTLG_SCHEDULE_PER_BLOCK;
-    if (letter_hit >= 0) {
-        found = true;
-        found_cost = c1;
-    }
-    for (cost = c1 + 1; cost <= max_cost; ++cost) {
-        if (on_the_fly) {
-            const int dif = cost - shortage;
-            if (dif == cf[1] || dif == c1 + cf[2] || dif == c1 + cf[3] || dif == cf[4] || dif == cf[5] ||
-                dif == cf[6] || dif == c1 + cf[7])
-                last_round = true;
-        }
-        std::vector<Block> blocks = level_blocks(cost, cf, opt->neg_type, ls);
-        // work items
-        const size_t nb = blocks.size();
-        if ((err = ensure(e->blocks, std::max<size_t>(nb, 1) * sizeof(BlockDesc))) != cudaSuccess ||
-            (err = ensure_host(e->h_blocks, std::max<size_t>(nb, 1) * sizeof(BlockDesc))) != cudaSuccess ||
-            (err = ensure(e->snaps, (std::max<size_t>(nb, 1) + 1) * sizeof(DevCtl))) != cudaSuccess ||
-            (err = ensure_host(e->h_snaps, (std::max<size_t>(nb, 1) + 1) * sizeof(DevCtl))) != cudaSuccess)
-            return fail_cuda(e, err, res);
-        BlockDesc *hb = (BlockDesc *)e->h_blocks.p;
-        long long items = 0;
-        uint64_t level_cands = 0;
-        for (const Block &B : blocks) level_cands += (uint64_t)B.candidates;
-        // Work-item size: a small level is cut into one right row (or one group of source
-        // rows) per warp so every SM takes part; a large level keeps the configured sizes.
-        {
-            const int nwarps = block_threads / 32;
-            if ((long long)level_cands < max_grid * 2048ll) {
-                A.right_chunk = nwarps;
-                A.unary_rows = nwarps * 4;
-            } else {
-                A.right_chunk = e->cfg.right_chunk;
-                A.unary_rows = e->cfg.unary_rows;
-            }
-        }
-        for (size_t b = 0; b < nb; ++b) {
-            const Block &B = blocks[b];
-            BlockDesc d{};
-            d.op = B.op;
-            d.l0 = B.l0;
-            d.l1 = B.l1;
-            d.r0 = B.r0;
-            d.r1 = B.r1;
-            d.item0 = items;
-            if (B.op == OP_AND || B.op == OP_OR || B.op == OP_U) {
-                const int tile = B.op == OP_U ? tl / 2 : tl;  // U: two candidates per pair
-                d.tiles_r = (B.r1 - B.r0 + A.right_chunk - 1) / A.right_chunk;
-                d.items = ((B.l1 - B.l0 + tile - 1) / tile) * d.tiles_r;
-            } else {
-                d.tiles_r = 1;
-                d.items = (B.r1 - B.r0 + A.unary_rows - 1) / A.unary_rows;
-            }
-            items += d.items;
-            hb[b] = d;
-        }
-        const long long stored_before = ls[cost];
-        // Items are numbered per operator (each operator's kernel drains its own queue);
-        // the per-block schedule numbers every block from 0.
-        {
-            long long op_items[7] = {0, 0, 0, 0, 0, 0, 0};
-            for (size_t b = 0; b < nb; ++b) {
-                const int op = hb[b].op;
-                hb[b].item0 = per_block ? 0 : op_items[op];
-                op_items[op] += hb[b].items;
-            }
-        }
-        if (nb) cudaMemcpyAsync(e->blocks.p, hb, nb * sizeof(BlockDesc), cudaMemcpyHostToDevice, st);
-        A.check_only = on_the_fly ? 1 : 0;
-        DevCtl *dctl = (DevCtl *)e->ctl.p;
-        if (!per_block && items > 0) cudaMemsetAsync(dctl->queue, 0, sizeof(dctl->queue), st);
+    const u32 fatal = ST_WAIT | ST_TMA | ST_TABLE;
+    auto fatal_status = [&](u32 f) { return (f & ST_TABLE) ? LTLG_TABLE_FULL : LTLG_DEVICE_WAIT; };
+
+    // ---- device-planned levels: per level a one-thread planner (plan from the level starts
+    // in device memory) and the level kernel, enqueued up to RING - 1 levels ahead of the
+    // level the host is reading, so the GPU never waits for the host between levels.
+    bool host_mode = per_block;
+    std::vector<float> level_ms;
+    if (!host_mode) {
+        constexpr int R = ltlg_engine::RING;
+        DevCtl *rctl = (DevCtl *)e->h_ring.p;
+        DevLevel *rlev = (DevLevel *)((char *)e->h_ring.p + R * sizeof(DevCtl));
+        int enq = 0, done = 0;
+        auto enqueue = [&]() -> cudaError_t {
+            const int k = enq % R;
+            cudaEventRecord(e->ev_start[k], st);
+            cudaError_t x = launch_plan(A, st);
+            if (x == cudaSuccess) x = launch_level(A, (int)max_grid, block_threads, st);
+            cudaEventRecord(e->ev_kend[k], st);
+            cudaMemcpyAsync(rctl + k, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
+            cudaMemcpyAsync(rlev + k, dlev, offsetof(DevLevel, blocks), cudaMemcpyDeviceToHost, st);
+            cudaEventRecord(e->ev_done[k], st);
+            launches += 2;
+            ++enq;
+            return x;
+        };
         cudaEventRecord(e->ev_a, st);
-        if (!per_block) {
-            if (items > 0) {
-                // fork: every operator with work runs concurrently on its own stream
-                cudaEventRecord(e->ev_fork, st);
-                size_t b = 0;
-                while (b < nb) {
-                    const int op = hb[b].op;
-                    size_t b2 = b;
-                    long long op_total = 0;
-                    while (b2 < nb && hb[b2].op == op) op_total += hb[b2++].items;
-                    A.blocks = (const BlockDesc *)e->blocks.p + b;
-                    A.nblocks = (int)(b2 - b);
-                    A.total_items = op_total;
-                    A.queue = dctl->queue + op;
-                    cudaStreamWaitEvent(e->op_stream[op], e->ev_fork, 0);
-                    const int grid = (int)std::min<long long>(op_total, max_grid_op[op]);
-                    if ((err = launch_op(op, A, grid, block_threads, e->op_stream[op])) != cudaSuccess)
-                        return fail_cuda(e, err, res);
-                    ++launches;
-                    cudaEventRecord(e->ev_join[op], e->op_stream[op]);
-                    cudaStreamWaitEvent(st, e->ev_join[op], 0);
-                    b = b2;
+        while (enq < R - 1 && c1 + enq < max_cost)
+            if ((err = enqueue()) != cudaSuccess) return fail_cuda(e, err, res);
+        while (done < enq) {
+            const int k = done % R;
+            if ((err = cudaEventSynchronize(e->ev_done[k])) != cudaSuccess) return fail_cuda(e, err, res);
+            ++done;
+            const DevCtl &sc = rctl[k];
+            const DevLevel &sl = rlev[k];
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e->ev_start[k], e->ev_kend[k]);
+            if (!sl.halt) level_ms.push_back(ms);
+            dflags |= sc.status;
+            bool stop = sl.halt != 0;
+            if (sc.status & fatal) {
+                status = fatal_status(sc.status);
+                stop = true;
+            } else if (sc.found && !found) {
+                found = true;
+                found_word = sc.found;
+                found_cost = (int)sc.found_cost;
+                if (opt->stop_at_found) {
+                    status = LTLG_FOUND;
+                    stop = true;
                 }
             }
-        } else {
-            for (size_t b = 0; b < nb; ++b) {
-                const int op = hb[b].op;
-                cudaMemcpyAsync((DevCtl *)e->snaps.p + b, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToDevice, st);
-                cudaMemsetAsync(dctl->queue + op, 0, sizeof(u64), st);
-                A.blocks = (const BlockDesc *)e->blocks.p + b;
-                A.nblocks = 1;
-                A.total_items = hb[b].items;
-                A.queue = dctl->queue + op;
-                const int grid = (int)std::min<long long>(hb[b].items, max_grid_op[op]);
-                if ((err = launch_op(op, A, grid, block_threads, st)) != cudaSuccess) return fail_cuda(e, err, res);
-                ++launches;
+            if (!stop && (sc.status & ST_OVERFLOW)) stop = true;
+            if (!sl.halt) last_cost = sl.cost;
+            if (sl.halt == 2) stop = true;
+            if (!stop && sl.cost >= max_cost) stop = true;
+            if (!stop && opt->time_limit_s > 0 && now_s() - t0 > opt->time_limit_s) {
+                status = LTLG_TIMEOUT;
+                stop = true;
             }
+            if (stop) break;
+            if (c1 + enq < max_cost)
+                if ((err = enqueue()) != cudaSuccess) return fail_cuda(e, err, res);
         }
         cudaEventRecord(e->ev_b, st);
         cudaMemcpyAsync(hc, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
-        if (per_block && nb)
-            cudaMemcpyAsync(e->h_snaps.p, e->snaps.p, nb * sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(hl, dlev, offsetof(DevLevel, blocks), cudaMemcpyDeviceToHost, st);
         if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
         float ms = 0;
         cudaEventElapsedTime(&ms, e->ev_a, e->ev_b);
         device_ms += ms;
         dflags |= hc->status;
-        const long long stored = std::min<long long>((long long)hc->row_count, cap_rows);
-        // Reference-style candidate counting: whole blocks up to the one holding the find.
-        uint64_t counted = level_cands;
-        size_t nb_reported = nb;
-        if (hc->found && !found) {
-            const u64 p = hc->found & ~(1ull << 63);
-            const int fop = parent_op(p);
-            const long long l = (long long)parent_left(p), r = (long long)parent_right(p);
-            int lc = cost_of_row(ls, l);
-            if (fop == OP_U) lc = std::min(lc, cost_of_row(ls, r));
-            counted = 0;
-            nb_reported = 0;
-            for (const Block &B : blocks) {
-                counted += (uint64_t)B.candidates;
-                ++nb_reported;
-                if (B.op == fop && B.lcost == lc) break;
+        if (status == LTLG_NOT_FOUND && !(hc->status & fatal) && ((hc->status & ST_OVERFLOW) || hl->halt == 2))
+            host_mode = true;
+        if (host_mode) {
+            if (hl->halt == 2) {
+                status = LTLG_BAD_ARGS;  // a level with more splits than a device plan holds
+                host_mode = false;
+            } else {
+                // the level that overflowed ran to its end; continue after it on the host
+                on_the_fly = true;
+                shortage = (int)hc->overflow_cost;
+                hl->cost = shortage;
+                hl->halt = 0;
+                hl->on_the_fly = 1;
+                cudaMemcpyAsync(dlev, hl, offsetof(DevLevel, blocks), cudaMemcpyHostToDevice, st);
             }
         }
-        if (per_block) {
-            const DevCtl *sn = (const DevCtl *)e->h_snaps.p;
-            uint64_t before = all;
-            for (size_t b = 0; b < nb_reported; ++b) {
-                ltlg_block_stat s{};
-                s.cost = cost;
-                s.op = blocks[b].op;
-                s.left_cost = blocks[b].lcost;
-                s.right_cost = blocks[b].rcost;
-                s.stored_before = std::min<long long>((long long)sn[b].row_count, cap_rows);
-                s.all_before = before;
-                s.to_check = blocks[b].candidates;
-                bstats.push_back(s);
-                before += (uint64_t)blocks[b].candidates;
+    }
+
+    // ---- host-driven levels: the per-block schedule (per-block statistics, the reference's
+    // progress lines) and the on-the-fly overflow regime (ltli6463.cu:1202-1206, 1442-1443).
+    if (host_mode && status == LTLG_NOT_FOUND && !(found && opt->stop_at_found)) {
+        uint64_t all_before = all;
+        for (;;) {
+            const int cost = hl->cost + 1;
+            if (cost > max_cost) {
+                last_cost = max_cost;
+                break;
             }
-        }
-        all += counted;
-        ltlg_level_stat L{};
-        L.cost = cost;
-        L.blocks = (int)nb;
-        L.candidates = level_cands;
-        L.uniques = (uint64_t)(stored - stored_before);
-        L.ms = ms;
-        lstats.push_back(L);
-        if (hc->status & (ST_WAIT | ST_TMA)) {
-            status = LTLG_DEVICE_WAIT;
-            break;
-        }
-        if (hc->status & ST_TABLE) {
-            status = LTLG_TABLE_FULL;
-            break;
-        }
-        if (hc->found && !found) {
-            found = true;
-            found_word = hc->found;
-            found_cost = cost;
-            if (opt->stop_at_found) {
-                ls[cost + 1] = stored;
-                status = LTLG_FOUND;
+            if (on_the_fly && shortage >= 0) {
+                const int dif = cost - shortage;
+                if (dif == cf[1] || dif == c1 + cf[2] || dif == c1 + cf[3] || dif == cf[4] || dif == cf[5] ||
+                    dif == cf[6] || dif == c1 + cf[7])
+                    last_round = true;
+            }
+            if ((err = launch_plan(A, st)) != cudaSuccess) return fail_cuda(e, err, res);
+            ++launches;
+            cudaMemcpyAsync(hl, dlev, sizeof(DevLevel), cudaMemcpyDeviceToHost, st);
+            cudaMemcpyAsync(hc, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
+            if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
+            if (hl->halt) {
+                if (hl->halt == 2) status = LTLG_BAD_ARGS;  // more splits than a plan holds
+                last_cost = std::min(cost, max_cost);
+                break;
+            }
+            cudaEventRecord(e->ev_a, st);
+            DevCtl *dctl = (DevCtl *)e->ctl.p;
+            if (per_block) {
+                // one launch per block in the reference's order, each after a snapshot
+                size_t nb_level = 0;
+                long long base = 0;
+                for (int op = 0; op < 7; ++op) {
+                    for (int k = 0; k < hl->nblocks[op]; ++k) {
+                        const BlockDesc &B = hl->blocks[op][k];
+                        cudaMemcpyAsync((DevCtl *)e->snaps.p + nb_level, e->ctl.p, sizeof(DevCtl),
+                                        cudaMemcpyDeviceToDevice, st);
+                        long long *win = (long long *)e->h_win.p + 2 * nb_level;
+                        win[0] = base + B.item0;
+                        win[1] = base + B.item0 + B.items;
+                        cudaMemcpyAsync(&dctl->queue[0], &win[0], sizeof(u64), cudaMemcpyHostToDevice, st);
+                        cudaMemcpyAsync(&dlev->item_hi_all, &win[1], sizeof(long long), cudaMemcpyHostToDevice, st);
+                        const int grid = (int)std::min<long long>(B.items, max_grid);
+                        if ((err = launch_level(A, grid, block_threads, st)) != cudaSuccess)
+                            return fail_cuda(e, err, res);
+                        ++launches;
+                        ++nb_level;
+                    }
+                    base += hl->total_items[op];
+                }
+            } else {
+                const int grid = (int)std::min<long long>(hl->item_hi_all, max_grid);
+                if (grid > 0) {
+                    if ((err = launch_level(A, grid, block_threads, st)) != cudaSuccess) return fail_cuda(e, err, res);
+                    ++launches;
+                }
+            }
+            cudaEventRecord(e->ev_b, st);
+            const u64 prev_rows = hc->row_count;
+            cudaMemcpyAsync(hc, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
+            size_t nsnap = 0;
+            for (int op = 0; op < 7; ++op) nsnap += (size_t)hl->nblocks[op];
+            if (per_block && nsnap)
+                cudaMemcpyAsync(e->h_snaps.p, e->snaps.p, nsnap * sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
+            if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
+            (void)prev_rows;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e->ev_a, e->ev_b);
+            device_ms += ms;
+            dflags |= hc->status;
+            if (per_block) {
+                const DevCtl *sn = (const DevCtl *)e->h_snaps.p;
+                size_t q = 0;
+                uint64_t before = all_before;
+                for (int op = 0; op < 7; ++op)
+                    for (int k = 0; k < hl->nblocks[op]; ++k, ++q) {
+                        const BlockDesc &B = hl->blocks[op][k];
+                        ltlg_block_stat sb{};
+                        sb.cost = cost;
+                        sb.op = op;
+                        sb.left_cost = B.lcost;
+                        sb.right_cost = (op == OP_AND || op == OP_OR || op == OP_U) ? cost - B.lcost - cf[op + 1] : 0;
+                        sb.stored_before = std::min<long long>((long long)sn[q].row_count, cap_rows);
+                        sb.all_before = before;
+                        sb.to_check = B.candidates;
+                        before += (uint64_t)B.candidates;
+                        bstats.push_back(sb);
+                    }
+                all_before = before;
+            }
+            if (hc->status & fatal) {
+                status = fatal_status(hc->status);
+                last_cost = cost;
+                break;
+            }
+            if (hc->found && !found) {
+                found = true;
+                found_word = hc->found;
+                found_cost = (int)hc->found_cost;
+                if (opt->stop_at_found) {
+                    status = LTLG_FOUND;
+                    break;
+                }
+            }
+            if (!on_the_fly && (hc->status & ST_OVERFLOW)) {
+                on_the_fly = true;
+                hl->on_the_fly = 1;
+                cudaMemcpyAsync(&dlev->on_the_fly, &hl->on_the_fly, sizeof(int), cudaMemcpyHostToDevice, st);
+            }
+            last_cost = cost;
+            if (last_round) break;
+            if (on_the_fly && shortage == -1) shortage = cost;
+            if (opt->time_limit_s > 0 && now_s() - t0 > opt->time_limit_s) {
+                status = LTLG_TIMEOUT;
                 break;
             }
         }
-        if (!on_the_fly) {
-            if (hc->status & ST_OVERFLOW) {
-                on_the_fly = true;
-                hc->row_count = (u64)cap_rows;
-            }
+    }
+
+    // ---- level ranges, statistics, reference-style candidate count
+    cudaMemcpyAsync(e->h_ls.p, e->ls.p, (MAX_COSTS + 2) * sizeof(long long), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(e->h_lcands.p, e->lcands.p, (MAX_COSTS + 2) * sizeof(u64), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hc, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
+    if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
+    const long long rows_final = std::min<long long>((long long)hc->row_count, cap_rows);
+    const long long *hls = (const long long *)e->h_ls.p;
+    const u64 *hlc = (const u64 *)e->h_lcands.p;
+    const int top = found && opt->stop_at_found ? found_cost : std::max(last_cost, c1);
+    std::vector<long long> &ls = e->level_start;
+    ls.assign((size_t)std::max(max_cost, c1) + 3, rows_final);
+    for (int k = 0; k <= c1 && k < (int)ls.size(); ++k) ls[k] = 0;
+    if (c1 + 1 < (int)ls.size()) ls[c1 + 1] = nalpha;
+    for (int k = c1 + 1; k <= std::min(top, MAX_COSTS) && k < (int)ls.size(); ++k) ls[k] = hls[k] > 0 ? hls[k] : ls[k];
+    for (int k = std::min(top, MAX_COSTS) + 1; k < (int)ls.size(); ++k) ls[k] = rows_final;
+    std::vector<ltlg_level_stat> lstats;
+    for (int c = c1 + 1; c <= top && c + 1 < (int)ls.size(); ++c) {
+        ltlg_level_stat L{};
+        L.cost = c;
+        L.candidates = c <= MAX_COSTS ? hlc[c] : 0;
+        L.uniques = (uint64_t)(ls[c + 1] - ls[c]);
+        const size_t i = (size_t)(c - c1 - 1);
+        L.ms = i < level_ms.size() ? level_ms[i] : 0.0;
+        lstats.push_back(L);
+    }
+    // all_ltls: whole levels before the found one, then the found level's blocks in the
+    // reference's order up to and including the block holding the find.
+    for (const auto &L : lstats)
+        if (!(found && opt->stop_at_found && L.cost == found_cost)) all += L.candidates;
+    if (found && opt->stop_at_found && found_word) {
+        const u64 p = found_word & ~(1ull << 63);
+        const int fop = parent_op(p);
+        int lc = cost_of_row(ls, (long long)parent_left(p));
+        if (fop == OP_U) lc = std::min(lc, cost_of_row(ls, (long long)parent_right(p)));
+        std::vector<Block> blocks = level_blocks(found_cost, cf, opt->neg_type, ls);
+        for (const Block &B : blocks) {
+            all += (uint64_t)B.candidates;
+            if (B.op == fop && B.lcost == lc) break;
         }
-        for (size_t k = (size_t)cost + 1; k < ls.size(); ++k) ls[k] = stored;
-        if (last_round) break;
-        if (on_the_fly && shortage == -1) shortage = cost;
-        if (opt->time_limit_s > 0 && now_s() - t0 > opt->time_limit_s) {
-            status = LTLG_TIMEOUT;
-            break;
+        if (per_block) {
+            // drop the blocks after the one holding the find
+            size_t keep = 0;
+            for (size_t i = 0; i < bstats.size(); ++i) {
+                keep = i + 1;
+                if (bstats[i].cost == found_cost && bstats[i].op == fop && bstats[i].left_cost == lc) break;
+            }
+            bstats.resize(keep);
         }
     }
-    if (cost == max_cost + 1) cost--;
     if (found && (status == LTLG_NOT_FOUND || status == LTLG_FOUND)) status = LTLG_FOUND;
     res->status = status;
-    res->cost = found ? found_cost : cost;
+    res->cost = found ? found_cost : last_cost;
     res->all_ltls = all;
     res->on_the_fly = on_the_fly ? 1 : 0;
     res->device_flags = dflags;
     res->device_ms = device_ms;
     res->evaluated = (uint64_t)nalpha + hc->evaluated;
-    res->rows = std::min<long long>((long long)hc->row_count, cap_rows);
+    res->rows = rows_final;
 
     std::string formula;
     if (letter_hit >= 0) {
         formula = std::string(1, alpha[letter_hit]);
         res->found_op = OP_ATOM;
-    } else if (found) {
-        const int cap = 1024;
-        if ((err = launch_walk((const u64 *)e->parents.p, nalpha, found_word, (u64 *)e->walk.p, cap, st)) !=
+    } else if (found && found_word) {
+        const int wcap = 1024;
+        if ((err = launch_walk((const u64 *)e->parents.p, nalpha, found_word, (u64 *)e->walk.p, wcap, st)) !=
             cudaSuccess)
             return fail_cuda(e, err, res);
         ++launches;
-        cudaMemcpyAsync(e->h_walk.p, e->walk.p, (2 + 2 * cap) * 8, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(e->h_walk.p, e->walk.p, (2 + 2 * wcap) * 8, cudaMemcpyDeviceToHost, st);
         if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
         const u64 *w = (const u64 *)e->h_walk.p;
         const u64 count = w[0], overflow = w[1];
@@ -759,6 +852,60 @@ LTLG_API int ltlg_learn(const ltlg_traces *t, const ltlg_options *opt, ltlg_resu
     }
     rc = ltlg_engine_learn(e, t, opt, res);
     ltlg_engine_destroy(e);
+    return rc;
+}
+
+struct ltlg_batch {
+    std::vector<ltlg_engine *> engines;
+};
+
+LTLG_API int ltlg_batch_create(const ltlg_engine_config *cfg, int32_t workers, ltlg_batch **out) {
+    *out = nullptr;
+    if (workers < 1 || workers > 64) return LTLG_BAD_ARGS;
+    auto *b = new ltlg_batch();
+    for (int w = 0; w < workers; ++w) {
+        ltlg_engine *e = nullptr;
+        const int rc = ltlg_engine_create(cfg, &e);
+        if (rc != 0) {
+            ltlg_batch_destroy(b);
+            return rc;
+        }
+        b->engines.push_back(e);
+    }
+    *out = b;
+    return 0;
+}
+
+LTLG_API void ltlg_batch_destroy(ltlg_batch *b) {
+    if (!b) return;
+    for (ltlg_engine *e : b->engines) ltlg_engine_destroy(e);
+    delete b;
+}
+
+LTLG_API void *ltlg_batch_stream(ltlg_batch *b, int32_t worker) {
+    if (!b || worker < 0 || worker >= (int)b->engines.size()) return nullptr;
+    return (void *)b->engines[worker]->stream;
+}
+
+LTLG_API int ltlg_batch_learn(ltlg_batch *b, const ltlg_traces *traces, int32_t count, const ltlg_options *opt,
+                              ltlg_result *results) {
+    if (!b || count < 0 || (count && (!traces || !results || !opt))) return LTLG_BAD_ARGS;
+    std::atomic<int> next{0};
+    auto work = [&](ltlg_engine *e) {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= count) return;
+            ltlg_engine_learn(e, &traces[i], opt, &results[i]);
+        }
+    };
+    const int workers = std::min<int>((int)b->engines.size(), std::max(count, 1));
+    std::vector<std::thread> th;
+    for (int w = 1; w < workers; ++w) th.emplace_back(work, b->engines[w]);
+    work(b->engines[0]);
+    for (auto &t : th) t.join();
+    int rc = 0;
+    for (int i = 0; i < count; ++i)
+        if (results[i].status != LTLG_FOUND && results[i].status != LTLG_NOT_FOUND && !rc) rc = results[i].status;
     return rc;
 }
 

@@ -361,8 +361,8 @@ __device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u
                 u32 f = FIELD_OVERFLOW;
                 if (myrow < cap)
                     f = (u32)(myrow + 1);
-                else
-                    atomicOr(&A.ctl->status, ST_OVERFLOW);
+                else if ((atomicOr(&A.ctl->status, ST_OVERFLOW) & ST_OVERFLOW) == 0u)
+                    atomicCAS(&A.ctl->overflow_cost, 0u, (u32)A.cost);
                 st_release(A.slots + idx, tagbits | genbits | f);
                 state = S_DONE;
             }
@@ -440,7 +440,7 @@ __device__ __forceinline__ void finish(const LevelArgs &A, const Gen &g, u64 (&h
     if (acc) {
         const int t = __ffs(acc) - 1;
         const u64 p = __shfl_sync(FULL, myparent, t);
-        if (lane == 0) atomicCAS(&A.ctl->found, 0ull, (1ull << 63) | p);
+        if (lane == 0 && atomicCAS(&A.ctl->found, 0ull, (1ull << 63) | p) == 0ull) A.ctl->found_cost = (u32)A.cost;
         if (A.stop_at_found) return;
     }
     if (A.check_only) return;
@@ -466,8 +466,9 @@ __device__ __forceinline__ bool found_stop(const LevelArgs &A) {
 }
 
 // ---------------------------------------------------------------- work items
+// Each operator path is compiled as its own function so registers are allocated per path.
 template <int OP, int HK>
-__device__ void unary_item(const LevelArgs &A, const BlockDesc &B, long long local, int warp, int nwarps, int lane,
+__device__ __noinline__ void unary_item(const LevelArgs &A, const BlockDesc &B, long long local, int warp, int nwarps, int lane,
                            u64 &evals) {
     const long long s_first = B.r0 + local * A.unary_rows;
     const long long s_end = min(B.r1, s_first + (long long)A.unary_rows);
@@ -582,7 +583,7 @@ __device__ void binary_row(const LevelArgs &A, const ulonglong2 *tile, int nl, l
 }
 
 template <int OP, int TL, int HK>
-__device__ bool binary_item(const LevelArgs &A, const BlockDesc &B, long long local, u64 *tile, u64 *bar,
+__device__ __noinline__ bool binary_item(const LevelArgs &A, const BlockDesc &B, long long local, u64 *tile, u64 *bar,
                             u32 &phase, int warp, int nwarps, int lane, u64 &evals) {
     constexpr int TLOP = OP == OP_U ? TL / 2 : TL;  // U makes two candidates per pair
     const long long tl = local / B.tiles_r, tr = local % B.tiles_r;
@@ -611,60 +612,189 @@ __device__ bool binary_item(const LevelArgs &A, const BlockDesc &B, long long lo
     return true;
 }
 
-// One operator's work items.  Binary kernels stage a left tile per item with a bulk
-// copy; unary kernels use no shared memory.
-template <int OP, int TL, int HK>
-__global__ void __launch_bounds__(256, (OP == OP_AND || OP == OP_OR || OP == OP_U) ? 3 : 4)
-    op_kernel(const __grid_constant__ LevelArgs A) {
-    constexpr bool BIN = OP == OP_AND || OP == OP_OR || OP == OP_U;
+// One level: every work item of every block of the plan in A.lev, drained through one
+// queue in the reference's operator order (~, &, |, X, F, G, U).
+template <int TL, int HK>
+__global__ void __launch_bounds__(256, 3) level_kernel(const __grid_constant__ LevelArgs A0) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     u64 *tile = reinterpret_cast<u64 *>(smem_raw);
+    __shared__ __align__(16) LevelArgs A;
     __shared__ __align__(8) u64 bar;
-    __shared__ long long s_item;
+    __shared__ long long s_item, s_hi, s_base[8];
+    __shared__ int s_halt, s_nblocks[8];
     __shared__ u64 s_evals;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     if (threadIdx.x == 0) {
-        if (BIN) {
-            mbar_init(&bar, 1);
-            fence_mbar_init();
+        A = A0;
+        const DevLevel *L = A.lev;
+        s_halt = L->halt;
+        s_hi = L->item_hi_all;
+        long long b = 0;
+        for (int op = 0; op < 7; ++op) {
+            s_base[op] = b;
+            s_nblocks[op] = L->nblocks[op];
+            b += L->total_items[op];
         }
+        s_base[7] = b;
+        A.cost = L->cost;
+        A.check_only = L->check_only;
+        A.right_chunk = L->right_chunk;
+        A.unary_rows = L->unary_rows;
+        mbar_init(&bar, 1);
+        fence_mbar_init();
         s_evals = 0;
     }
     __syncthreads();
+    if (s_halt || s_hi <= 0) return;
     u32 phase = 0;
     u64 evals = 0;
     for (;;) {
         if (threadIdx.x == 0) {
             long long it = -1;
             if (!found_stop(A)) {
-                it = (long long)atomicAdd(A.queue, 1ull);
-                if (it >= A.total_items) it = -1;
+                it = (long long)atomicAdd(&A.ctl->queue[0], 1ull);
+                if (it >= s_hi) it = -1;
             }
             s_item = it;
         }
         __syncthreads();
         const long long item = s_item;
         if (item < 0) break;
-        int lo = 0, hi = A.nblocks - 1;
+        int op = 0;
+        while (op < 6 && item >= s_base[op + 1]) ++op;
+        const long long in_op = item - s_base[op];
+        const BlockDesc *blocks = A.lev->blocks[op];
+        int lo = 0, hi = s_nblocks[op] - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (A.blocks[mid].item0 <= item)
+            if (blocks[mid].item0 <= in_op)
                 lo = mid;
             else
                 hi = mid - 1;
         }
-        const BlockDesc B = A.blocks[lo];
-        const long long local = item - B.item0;
-        if (BIN) {
-            if (!binary_item<OP, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals)) break;
-        } else {
-            unary_item<OP, HK>(A, B, local, warp, nwarps, lane, evals);
+        const BlockDesc B = blocks[lo];
+        const long long local = in_op - B.item0;
+        bool ok = true;
+        switch (op) {
+        case OP_NEG: unary_item<OP_NEG, HK>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_X: unary_item<OP_X, HK>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_F: unary_item<OP_F, HK>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_G: unary_item<OP_G, HK>(A, B, local, warp, nwarps, lane, evals); break;
+        case OP_AND: ok = binary_item<OP_AND, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
+        case OP_OR: ok = binary_item<OP_OR, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
+        default: ok = binary_item<OP_U, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
         }
+        if (!ok) break;
         __syncthreads();
     }
     if (lane == 0 && evals) atomicAdd(&s_evals, evals);
     __syncthreads();
     if (threadIdx.x == 0 && s_evals) atomicAdd(&A.ctl->evaluated, s_evals);
+}
+
+// The planner: one thread turns the level starts into the next level's plan, in the
+// reference's order (ltli6463.cu:1209-1440; NegType rule :1212): ~, & splits, | splits,
+// X, F, G, U splits; a split i pairs cost i with cost c - i - c_op, i = c1 .. (c - c_op)/2.
+__global__ void plan_kernel(const __grid_constant__ LevelArgs A) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    DevLevel *L = A.lev;
+    DevCtl *C = A.ctl;
+    if (L->halt == 2) return;  // an over-long plan stops the rest of the graph
+    const int c = L->cost + 1;
+    L->cost = c;
+    const long long rows = min((long long)C->row_count, A.cap_rows);
+    if (c < MAX_COSTS + 1) A.ls[c] = rows;  // level c - 1 ended here
+    u32 bad = ST_WAIT | ST_TABLE | ST_TMA;
+    if (!L->on_the_fly) bad |= ST_OVERFLOW;
+    const bool halt = c > A.max_cost || c >= MAX_COSTS || (A.stop_at_found && C->found != 0ull) ||
+                      (C->status & bad) != 0u;
+    for (int k = 0; k < 8; ++k) {
+        L->nblocks[k] = 0;
+        L->total_items[k] = 0;
+        L->item_hi[k] = 0;
+        C->queue[k] = 0;
+    }
+    L->item_lo = 0;
+    L->item_hi_all = 0;
+    L->halt = halt ? 1 : 0;
+    L->level_cands = 0;
+    if (halt) return;
+    const int c1 = A.cf[0];
+    auto lo = [&](int k) { return (k >= 0 && k < c) ? A.ls[k] : 0ll; };
+    auto hi = [&](int k) { return (k >= 0 && k < c) ? A.ls[k + 1] : 0ll; };
+    u64 cands = 0;
+    bool overfull = false;
+    auto add = [&](int op, int lc, long long l0, long long l1, long long r0, long long r1, long long n) {
+        const int k = L->nblocks[op];
+        if (k >= MAX_SPLITS) {
+            overfull = true;
+            return;
+        }
+        BlockDesc &b = L->blocks[op][k];
+        b.op = op;
+        b.lcost = lc;
+        b.l0 = l0;
+        b.l1 = l1;
+        b.r0 = r0;
+        b.r1 = r1;
+        b.candidates = n;
+        L->nblocks[op] = k + 1;
+        cands += (u64)n;
+    };
+    auto unary = [&](int op, int k) {
+        const long long a = lo(k), b = hi(k);
+        if (b > a) add(op, k, 0, 0, a, b, b - a);
+    };
+    auto binary = [&](int op, int cop) {
+        for (int i = c1; 2 * i <= c - cop; ++i) {
+            const int j = c - i - cop;
+            const long long a = lo(i), b = hi(i), x = lo(j), y = hi(j);
+            if (b > a && y > x) add(op, i, a, b, x, y, (op == OP_U ? 2 : 1) * (b - a) * (y - x));
+        }
+    };
+    const int *cf = A.cf;
+    if ((A.neg_type == 1 && c - cf[1] >= c1) || (A.neg_type == 2 && c - cf[1] == c1)) unary(OP_NEG, c - cf[1]);
+    binary(OP_AND, cf[2]);
+    binary(OP_OR, cf[3]);
+    if (c - cf[4] >= c1) unary(OP_X, c - cf[4]);
+    if (c - cf[5] >= c1) unary(OP_F, c - cf[5]);
+    if (c - cf[6] >= c1) unary(OP_G, c - cf[6]);
+    binary(OP_U, cf[7]);
+    if (overfull) {  // more splits than a plan holds: hand the level back to the host
+        for (int k = 0; k < 8; ++k) L->nblocks[k] = 0;
+        L->halt = 2;
+        return;
+    }
+    // Work-item size: a small level is cut into one right row (or one group of source rows)
+    // per warp so every SM takes part; a large level keeps the configured sizes.
+    const bool small = (long long)cands < A.small_level;
+    const int rc = small ? A.nwarps : A.right_chunk_big;
+    const int ur = small ? A.nwarps * UNARY_GROUP : A.unary_rows_big;
+    L->right_chunk = rc;
+    L->unary_rows = ur;
+    L->check_only = L->on_the_fly;
+    L->level_cands = cands;
+    if (c < MAX_COSTS + 1) A.level_cands[c] = cands;
+    for (int op = 0; op < 7; ++op) {
+        long long items = 0;
+        const bool bin = op == OP_AND || op == OP_OR || op == OP_U;
+        const int tile = op == OP_U ? A.left_tile / 2 : A.left_tile;
+        for (int k = 0; k < L->nblocks[op]; ++k) {
+            BlockDesc &b = L->blocks[op][k];
+            b.item0 = items;
+            if (bin) {
+                b.tiles_r = (b.r1 - b.r0 + rc - 1) / rc;
+                b.items = ((b.l1 - b.l0 + tile - 1) / tile) * b.tiles_r;
+            } else {
+                b.tiles_r = 1;
+                b.items = (b.r1 - b.r0 + ur - 1) / ur;
+            }
+            items += b.items;
+        }
+        L->total_items[op] = items;
+        L->item_hi[op] = items;
+        L->item_hi_all += items;
+    }
 }
 
 // Letters: register rows [0, nalpha) in the hash set (duplicate letters stay rows,
@@ -820,79 +950,51 @@ __global__ void apply_op_kernel(int op, const u64 *a, const u64 *b, const u64 *w
 
 }  // namespace
 
-int op_kernel_smem_bytes(int op, int left_tile, int pitch) {
-    if (op == OP_AND || op == OP_OR) return left_tile * pitch * 8;
-    if (op == OP_U) return (left_tile / 2) * pitch * 8;
-    return 0;
+int level_kernel_smem_bytes(int left_tile, int pitch) { return left_tile * pitch * 8; }
+
+template <int TL, int HK>
+static cudaError_t smem_attr(int smem) {
+    static int attr_set = 48 * 1024;  // largest dynamic shared memory size enabled so far
+    if (smem <= attr_set) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(level_kernel<TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) attr_set = smem;
+    return e;
 }
 
-template <int OP, int TL, int HK>
-static cudaError_t launch_one(const LevelArgs &a, int grid, int block, cudaStream_t s) {
-    const int smem = op_kernel_smem_bytes(OP, TL, a.pitch);
-    static int attr_set = -1;  // largest dynamic shared memory size enabled so far
-    if (smem > 48 * 1024 && smem > attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(op_kernel<OP, TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr_set = smem;
-    }
-    op_kernel<OP, TL, HK><<<grid, block, smem, s>>>(a);
+template <int TL, int HK>
+static cudaError_t launch_tl(const LevelArgs &a, int grid, int block, cudaStream_t s) {
+    const int smem = level_kernel_smem_bytes(TL, a.pitch);
+    cudaError_t e = smem_attr<TL, HK>(smem);
+    if (e != cudaSuccess) return e;
+    level_kernel<TL, HK><<<grid, block, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-template <int OP, int TL, int HK>
-static int occupancy_one(int block, int pitch) {
-    const int smem = op_kernel_smem_bytes(OP, TL, pitch);
+template <int TL, int HK>
+static int occupancy_tl(int block, int pitch) {
+    const int smem = level_kernel_smem_bytes(TL, pitch);
+    if (smem_attr<TL, HK>(smem) != cudaSuccess) return 0;
     int n = 0;
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(op_kernel<OP, TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, op_kernel<OP, TL, HK>, block, smem) == cudaSuccess ? n
-                                                                                                                : 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<TL, HK>, block, smem) == cudaSuccess ? n : 0;
 }
 
-template <int TL, int HK>
-static cudaError_t launch_tl(int op, const LevelArgs &a, int grid, int block, cudaStream_t s) {
-    switch (op) {
-    case OP_NEG: return launch_one<OP_NEG, TL, HK>(a, grid, block, s);
-    case OP_AND: return launch_one<OP_AND, TL, HK>(a, grid, block, s);
-    case OP_OR: return launch_one<OP_OR, TL, HK>(a, grid, block, s);
-    case OP_X: return launch_one<OP_X, TL, HK>(a, grid, block, s);
-    case OP_F: return launch_one<OP_F, TL, HK>(a, grid, block, s);
-    case OP_G: return launch_one<OP_G, TL, HK>(a, grid, block, s);
-    case OP_U: return launch_one<OP_U, TL, HK>(a, grid, block, s);
-    default: return cudaErrorInvalidValue;
-    }
+cudaError_t launch_level(const LevelArgs &a, int grid, int block, cudaStream_t s) {
+    if (a.hash_kind == 1) return a.left_tile == 4 ? launch_tl<4, 1>(a, grid, block, s) : launch_tl<8, 1>(a, grid, block, s);
+    return a.left_tile == 4 ? launch_tl<4, 0>(a, grid, block, s) : launch_tl<8, 0>(a, grid, block, s);
 }
 
-template <int TL, int HK>
-static int occupancy_tl(int op, int block, int pitch) {
-    switch (op) {
-    case OP_NEG: return occupancy_one<OP_NEG, TL, HK>(block, pitch);
-    case OP_AND: return occupancy_one<OP_AND, TL, HK>(block, pitch);
-    case OP_OR: return occupancy_one<OP_OR, TL, HK>(block, pitch);
-    case OP_X: return occupancy_one<OP_X, TL, HK>(block, pitch);
-    case OP_F: return occupancy_one<OP_F, TL, HK>(block, pitch);
-    case OP_G: return occupancy_one<OP_G, TL, HK>(block, pitch);
-    case OP_U: return occupancy_one<OP_U, TL, HK>(block, pitch);
-    default: return 0;
-    }
+int level_kernel_max_ctas_per_sm(int left_tile, int hash_kind, int block, int pitch) {
+    if (hash_kind == 1) return left_tile == 4 ? occupancy_tl<4, 1>(block, pitch) : occupancy_tl<8, 1>(block, pitch);
+    return left_tile == 4 ? occupancy_tl<4, 0>(block, pitch) : occupancy_tl<8, 0>(block, pitch);
 }
 
-cudaError_t launch_op(int op, const LevelArgs &a, int grid, int block, cudaStream_t s) {
-    if (a.key_mode == KEY_HASH64) {
-        if (a.left_tile == 4) return launch_tl<4, 1>(op, a, grid, block, s);
-        return launch_tl<8, 1>(op, a, grid, block, s);
-    }
-    if (a.left_tile == 4) return launch_tl<4, 0>(op, a, grid, block, s);
-    return launch_tl<8, 0>(op, a, grid, block, s);
-}
-
-int op_kernel_max_ctas_per_sm(int op, int left_tile, int hash_kind, int block, int pitch) {
-    if (hash_kind == 1) return left_tile == 4 ? occupancy_tl<4, 1>(op, block, pitch) : occupancy_tl<8, 1>(op, block, pitch);
-    return left_tile == 4 ? occupancy_tl<4, 0>(op, block, pitch) : occupancy_tl<8, 0>(op, block, pitch);
+cudaError_t launch_plan(const LevelArgs &a, cudaStream_t s) {
+    plan_kernel<<<1, 32, 0, s>>>(a);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_insert_letters(const LevelArgs &a, int nalpha, cudaStream_t s) {
-    if (a.key_mode == KEY_HASH64)
+    if (a.hash_kind == 1)
         insert_letters_kernel<1><<<1, 32, 0, s>>>(a, nalpha);
     else
         insert_letters_kernel<0><<<1, 32, 0, s>>>(a, nalpha);

@@ -34,6 +34,8 @@ struct DevCtl {
     u64 found;       // 0, or (1 << 63) | parents of an accepting candidate
     u64 evaluated;   // candidates evaluated
     u32 status;      // ST_* bits
+    u32 found_cost;  // level at which `found` was set
+    u32 overflow_cost;  // level at which the cache first overflowed
     u32 pad;
     u64 queue[8];    // next work item of each operator's kernel
 };
@@ -42,21 +44,53 @@ struct DevCtl {
 // Binary: left rows [l0, l1) x right rows [r0, r1).
 struct BlockDesc {
     int op;
-    int pad;
+    int lcost;           // cost of the left operand (unary: of the operand)
     long long l0, l1, r0, r1;
-    long long item0;     // first work item of this block
+    long long item0;     // first work item of this block within its operator
     long long items;     // work items of this block
     long long tiles_r;   // binary: right chunks per left tile
+    long long candidates;  // as the reference counts them (U: two per pair)
+};
+
+constexpr int MAX_SPLITS = 64;   // blocks per operator and level in a device-planned level
+constexpr int MAX_COSTS = 512;   // level starts kept on the device
+
+// The plan of the level being enumerated, in device memory.  The planner kernel writes it
+// from the level starts; the host writes it directly in the per-block schedule.
+struct DevLevel {
+    int cost;            // the level being enumerated (the planner advances it)
+    int halt;            // 1: every operator kernel of this level exits at once
+    int check_only;      // on-the-fly: acceptance only, no dedupe, no storing
+    int on_the_fly;      // set by the host: plan check-only levels and ignore the overflow bit
+    long long item_lo;   // the level kernel takes items from ctl->queue[0] in [item_lo, item_hi_all)
+    long long item_hi_all;
+    int right_chunk;
+    int unary_rows;
+    int nblocks[8];
+    long long total_items[8];
+    long long item_hi[8];  // an operator kernel takes items from its queue until item_hi
+    u64 level_cands;     // candidates of the level, counted as the reference counts them
+    BlockDesc blocks[7][MAX_SPLITS];
 };
 
 struct LevelArgs {
-    const BlockDesc *blocks;  // this operator's blocks
-    u64 *queue;               // this operator's work-item counter
-    int nblocks;
+    // constant during a learn
     int n;               // traces = words per CS
     int pitch;           // words per cache row (n rounded up to a multiple of 4)
     int npos;
-    long long total_items;
+    int nalpha;
+    int key_mode;
+    int rlx_type;        // KEY_REF: 0 exact pack, 1, 2, 3
+    u32 gen;             // hash-set generation (1..255)
+    int stop_at_found;
+    int left_tile;
+    int neg_type;
+    int max_cost;
+    int nwarps;
+    int cf[8];           // costs of p ~ & | X F G U
+    int right_chunk_big, unary_rows_big;
+    int hash_kind;       // fingerprint kind of the operator kernels (0 multiply-add, 1 fmix64)
+    long long small_level;  // levels with fewer candidates use one row per warp per item
     long long cap_rows;
     u64 *cache;
     u64 *parents;
@@ -66,21 +100,22 @@ struct LevelArgs {
     const u64 *wmeta;    // per word: length mask | (positive << 63); 0 for padding
     const u32 *kmeta;    // KEY_REF: per word start | count << 16 | step << 24
     DevCtl *ctl;
-    int key_mode;
-    int rlx_type;        // KEY_REF: 0 exact pack, 1, 2, 3
-    u32 gen;             // hash-set generation (1..255)
-    int stop_at_found;
-    int check_only;      // on-the-fly: acceptance only, no dedupe, no storing
+    DevLevel *lev;
+    long long *ls;       // level starts: rows of cost c are [ls[c], ls[c + 1])
+    u64 *level_cands;    // per cost
+    // per level (filled into the shared copy from the plan)
+    int cost;
+    int check_only;
     int right_chunk;
     int unary_rows;
-    int left_tile;
 };
 
-// Launch wrappers (ltl_kernels.cu).  One kernel per operator drains the work items of
-// that operator's blocks; binary kernels stage left tiles of left_tile rows (U: half).
-int op_kernel_smem_bytes(int op, int left_tile, int pitch);
-cudaError_t launch_op(int op, const LevelArgs &a, int grid, int block, cudaStream_t s);
-int op_kernel_max_ctas_per_sm(int op, int left_tile, int hash_kind, int block, int pitch);
+// Launch wrappers (ltl_kernels.cu).  The level kernel drains the work items of every block
+// of the planned level; binary items stage left tiles of left_tile rows (U: half).
+int level_kernel_smem_bytes(int left_tile, int pitch);
+int level_kernel_max_ctas_per_sm(int left_tile, int hash_kind, int block, int pitch);
+cudaError_t launch_level(const LevelArgs &a, int grid, int block, cudaStream_t s);
+cudaError_t launch_plan(const LevelArgs &a, cudaStream_t s);
 cudaError_t launch_insert_letters(const LevelArgs &a, int nalpha, cudaStream_t s);
 cudaError_t launch_walk(const u64 *parents, int nalpha, u64 found, u64 *out, int cap, cudaStream_t s);
 cudaError_t launch_apply_op(int op, const u64 *a, const u64 *b, const u64 *wmeta, int n, int pitch, int count,

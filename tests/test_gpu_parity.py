@@ -203,3 +203,13 @@ def test_gpu_matches_reference_outputs(engine, run):
         assert res.status == api.FOUND
         assert O.separates(res.formula, inst)
         assert O.formula_cost(res.formula, run["costs"]) == fin["cost"]
+
+
+def test_batch_learn_matches_single_engine():
+    insts = [gen.generate(2000 + s, 3, 40, 40, 5, 20, 0.5, 6) for s in range(16)]
+    with api.Batch(workers=4, slots_log2=22, cache_bytes=1 << 30, max_rows=1 << 20) as pool:
+        res = pool.learn(insts, neg_type=1)
+    for inst, r in zip(insts, res):
+        ref = O.learn(inst, neg_type=1)
+        assert r.status == api.FOUND and r.cost == ref.cost
+        assert O.separates(r.formula, inst)

@@ -177,6 +177,19 @@ LTLG_API int ltlg_batch_learn(ltlg_batch *b, const ltlg_traces *traces, int32_t 
 /* Stream of worker w's engine (for event timing around batch calls). */
 LTLG_API void *ltlg_batch_stream(ltlg_batch *b, int32_t worker);
 
+/* Learn without allocating: no counterpart in the reference.  For callers that cannot
+ * allocate device memory (GPU memory owned by another allocator, or no cudaMalloc allowed
+ * after start-up): every device buffer lives in one static 64 MiB array that the library
+ * holds on each GPU until exit, and host work uses stack arrays.  At most 64 traces of at
+ * most 63 steps (more: LTLG_INPUT_LIMITS); exact or 64-bit-fingerprint keys; a level that
+ * overflows the scratch returns LTLG_NO_MEMORY.  The formula is written to the caller's
+ * buffer (formula_cap bytes), the cost and candidate count to *cost and *all_ltls.  All
+ * calls share the array: calls whose GPU work overlaps race, so callers serialise them.
+ * The first call on a device looks up the array's address there; make it before any
+ * stream capture. */
+LTLG_API int ltlg_learn_noalloc(const ltlg_traces *traces, const ltlg_options *opt, char *formula,
+                                int32_t formula_cap, int32_t *cost, uint64_t *all_ltls);
+
 /* After a learn: copy cache rows [first, first + count) (n words each, pitch dropped) and
  * their packed parents (op << 60 | left << 30 | right) to host memory.  Either pointer may
  * be NULL.  Returns 0 or an ltlg_status. */

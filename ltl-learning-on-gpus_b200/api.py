@@ -29,7 +29,7 @@ EXPORTED = [
     "ltlg_engine_create", "ltlg_engine_destroy", "ltlg_engine_learn", "ltlg_learn", "ltlg_result_free",
     "ltlg_engine_read_rows", "ltlg_engine_level_starts", "ltlg_device_apply_op", "ltlg_read_scarlet",
     "ltlg_traces_free", "ltlg_engine_stream", "ltlg_batch_create", "ltlg_batch_destroy", "ltlg_batch_learn",
-    "ltlg_batch_stream",
+    "ltlg_batch_stream", "ltlg_learn_noalloc",
 ]
 
 

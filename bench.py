@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--max-cost", type=int, default=500)
     ap.add_argument("--no-stop", action="store_true", help="enumerate every level up to --max-cost")
     ap.add_argument("--cache-gb", type=float, default=6.0, help="language cache per engine")
-    ap.add_argument("--workers", type=int, default=8, help="engines of the batch call")
+    ap.add_argument("--workers", type=int, default=8,
+                    help="engines of the batch call; 0 times the single engine only (profiling runs)")
     ap.add_argument("--slots-log2", type=int, default=27)
     ap.add_argument("--cpu-sample-s", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -221,15 +222,19 @@ def run_ours(a):
     batch = make_batch(seeds_of(a.seeds, rank))
     ekw = dict(device=local, slots_log2=a.slots_log2, cache_bytes=int(a.cache_gb * (1 << 30)))
     eng = api.Engine(**ekw)
-    pool = api.Batch(workers=a.workers, **ekw)
+    pool = api.Batch(workers=a.workers, **ekw) if a.workers > 0 else None
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     opts = dict(neg_type=1, max_cost=a.max_cost, stop_at_found=not a.no_stop)
 
     def seq_step():
         return [eng.learn(inst, **opts) for inst in batch]
 
+    def batch_step():
+        return pool.learn(batch, **opts) if pool else seq_step()
+
     for _ in range(a.warmup):
-        pool.learn(batch, **opts)
+        if pool:
+            pool.learn(batch, **opts)
         seq_step()
     torch.cuda.synchronize()
 
@@ -250,7 +255,7 @@ def run_ours(a):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            res = pool.learn(batch, **opts)  # blocks until every engine's stream is idle
+            res = batch_step()  # blocks until every engine's stream is idle
             e1.record()
             torch.cuda.synchronize()
             barrier()
@@ -266,7 +271,7 @@ def run_ours(a):
                 d2h += len(r.formula) + 64
             flush.fill_(2)
             torch.cuda.synchronize()
-            seq = seq_step()
+            seq = seq_step() if pool else res
             kern_ms.append(sum(r.device_ms for r in seq))
             for inst, r in zip(batch, seq):
                 uniq_seq += r.rows - len(inst.alphabet)
@@ -317,7 +322,8 @@ def run_ours(a):
         if ws == 1 and not a.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(batch, a.cpu_sample_s)
         print(json.dumps(line), flush=True)
-    pool.close()
+    if pool:
+        pool.close()
     eng.close()
     if ws > 1:
         import torch.distributed as D

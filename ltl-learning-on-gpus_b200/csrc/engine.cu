@@ -66,9 +66,15 @@ struct ltlg_engine {
     int num_sms = 0;
     cudaStream_t stream = nullptr;
     static constexpr int RING = 4;     // levels in flight: the host runs up to RING - 1 ahead
-    cudaEvent_t ev_start[RING] = {}, ev_kend[RING] = {}, ev_done[RING] = {};
+    cudaEvent_t ev_start[RING] = {}, ev_done[RING] = {};
     cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
-    DevBuf cache, parents, keys, slots, wmeta, kmeta, ctl, walk, snaps, lev, ls, lcands;
+    DevBuf cache, parents, keys, slots, wmeta, kmeta, ctl, walk, snaps, lev, ls, lcands, args;
+    // One graph per ring slot: planner, level kernel, and the copy of the level's control
+    // block and plan header into that slot.  The kernels read their
+    // arguments from `args`, so the graphs stay valid from one learn to the next; they are
+    // captured again only when the kernel instances or grids change (graph_key).
+    cudaGraphExec_t level_graph[RING] = {};
+    long long graph_key[8] = {};
     DevBuf h_ctl, h_walk, h_stage, h_snaps, h_args, h_lev, h_ls, h_lcands, h_win, h_ring;
 
     u64 nslots = 0;
@@ -235,8 +241,7 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
     for (int k = 0; k < ltlg_engine::RING && err == cudaSuccess; ++k) {
         err = cudaEventCreate(&e->ev_start[k]);
-        if (err == cudaSuccess) err = cudaEventCreate(&e->ev_kend[k]);
-        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_done[k], cudaEventDisableTiming);
+        if (err == cudaSuccess) err = cudaEventCreate(&e->ev_done[k]);
     }
     if (err == cudaSuccess) err = cudaEventCreate(&e->ev_a);
     if (err == cudaSuccess) err = cudaEventCreate(&e->ev_b);
@@ -253,8 +258,9 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
     const size_t max_blocks = 7 * MAX_SPLITS;
     if (err == cudaSuccess) err = ensure(e->snaps, max_blocks * sizeof(DevCtl));
     if (err == cudaSuccess) err = ensure_host(e->h_snaps, max_blocks * sizeof(DevCtl));
-    if (err == cudaSuccess) err = ensure_host(e->h_win, max_blocks * 2 * sizeof(long long));
+    if (err == cudaSuccess) err = ensure_host(e->h_win, max_blocks * 8 * sizeof(long long));
     if (err == cudaSuccess) err = ensure_host(e->h_args, sizeof(LevelArgs));
+    if (err == cudaSuccess) err = ensure(e->args, sizeof(LevelArgs));
     if (err == cudaSuccess) err = ensure_host(e->h_ring, ltlg_engine::RING * (sizeof(DevCtl) + sizeof(DevLevel)));
     if (err == cudaSuccess) err = ensure(e->lev, sizeof(DevLevel));
     if (err == cudaSuccess) err = ensure_host(e->h_lev, sizeof(DevLevel));
@@ -275,8 +281,10 @@ LTLG_API void ltlg_engine_destroy(ltlg_engine *e) {
     if (!e) return;
     cudaSetDevice(e->cfg.device);
     if (e->stream) cudaStreamSynchronize(e->stream);
+    for (cudaGraphExec_t g : e->level_graph)
+        if (g) cudaGraphExecDestroy(g);
     for (DevBuf *b : {&e->cache, &e->parents, &e->keys, &e->slots, &e->wmeta, &e->kmeta, &e->ctl, &e->walk, &e->snaps,
-                      &e->lev, &e->ls, &e->lcands})
+                      &e->lev, &e->ls, &e->lcands, &e->args})
         if (b->p) cudaFree(b->p);
     for (DevBuf *b : {&e->h_ctl, &e->h_walk, &e->h_stage, &e->h_snaps, &e->h_args, &e->h_lev, &e->h_ls, &e->h_lcands,
                       &e->h_win, &e->h_ring})
@@ -284,7 +292,7 @@ LTLG_API void ltlg_engine_destroy(ltlg_engine *e) {
     for (cudaEvent_t ev : {e->ev_a, e->ev_b, e->ev_t0, e->ev_t1})
         if (ev) cudaEventDestroy(ev);
     for (int k = 0; k < ltlg_engine::RING; ++k)
-        for (cudaEvent_t ev : {e->ev_start[k], e->ev_kend[k], e->ev_done[k]})
+        for (cudaEvent_t ev : {e->ev_start[k], e->ev_done[k]})
             if (ev) cudaEventDestroy(ev);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
@@ -462,6 +470,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     }
     const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
     const int block_threads = e->cfg.block_threads;
+    // resident CTAs of the level kernel on all SMs
     const long long max_grid =
         (long long)e->num_sms * std::max(1, level_kernel_max_ctas_per_sm(tl, hk, block_threads, pitch));
 
@@ -505,7 +514,9 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     memset(hl, 0, offsetof(DevLevel, blocks));
     hl->cost = c1;  // the planner advances to c1 + 1 first
     cudaMemcpyAsync(dlev, hl, offsetof(DevLevel, blocks), cudaMemcpyHostToDevice, st);
-    if ((err = launch_insert_letters(A, nalpha, st)) != cudaSuccess) return fail_cuda(e, err, res);
+    const LevelArgs *dA = (const LevelArgs *)e->args.p;
+    cudaMemcpyAsync(e->args.p, ha, sizeof(LevelArgs), cudaMemcpyHostToDevice, st);
+    if ((err = launch_insert_letters(A, dA, nalpha, st)) != cudaSuccess) return fail_cuda(e, err, res);
     int launches = 1;
 
     int status = LTLG_NOT_FOUND;
@@ -529,14 +540,31 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         DevCtl *rctl = (DevCtl *)e->h_ring.p;
         DevLevel *rlev = (DevLevel *)((char *)e->h_ring.p + R * sizeof(DevCtl));
         int enq = 0, done = 0;
+        const long long key[8] = {tl, hk, pitch, block_threads, max_grid, 2, 0, 0};
+        if (memcmp(key, e->graph_key, sizeof(key)) != 0) {
+            memset(e->graph_key, 0, sizeof(e->graph_key));
+            for (int k = 0; k < R && err == cudaSuccess; ++k) {
+                if (e->level_graph[k]) cudaGraphExecDestroy(e->level_graph[k]);
+                e->level_graph[k] = nullptr;
+                cudaGraph_t g = nullptr;
+                err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+                if (err != cudaSuccess) break;
+                cudaError_t x = launch_plan(dA, st);
+                if (x == cudaSuccess) x = launch_level(A, dA, (int)max_grid, block_threads, st);
+                cudaMemcpyAsync(rctl + k, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(rlev + k, dlev, offsetof(DevLevel, blocks), cudaMemcpyDeviceToHost, st);
+                err = cudaStreamEndCapture(st, &g);
+                if (err == cudaSuccess) err = x;
+                if (err == cudaSuccess) err = cudaGraphInstantiate(&e->level_graph[k], g, 0);
+                if (g) cudaGraphDestroy(g);
+            }
+            if (err != cudaSuccess) return fail_cuda(e, err, res);
+            memcpy(e->graph_key, key, sizeof(key));
+        }
         auto enqueue = [&]() -> cudaError_t {
             const int k = enq % R;
             cudaEventRecord(e->ev_start[k], st);
-            cudaError_t x = launch_plan(A, st);
-            if (x == cudaSuccess) x = launch_level(A, (int)max_grid, block_threads, st);
-            cudaEventRecord(e->ev_kend[k], st);
-            cudaMemcpyAsync(rctl + k, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(rlev + k, dlev, offsetof(DevLevel, blocks), cudaMemcpyDeviceToHost, st);
+            const cudaError_t x = cudaGraphLaunch(e->level_graph[k], st);
             cudaEventRecord(e->ev_done[k], st);
             launches += 2;
             ++enq;
@@ -552,7 +580,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
             const DevCtl &sc = rctl[k];
             const DevLevel &sl = rlev[k];
             float ms = 0;
-            cudaEventElapsedTime(&ms, e->ev_start[k], e->ev_kend[k]);
+            cudaEventElapsedTime(&ms, e->ev_start[k], e->ev_done[k]);
             if (!sl.halt) level_ms.push_back(ms);
             dflags |= sc.status;
             bool stop = sl.halt != 0;
@@ -622,7 +650,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
                     dif == cf[6] || dif == c1 + cf[7])
                     last_round = true;
             }
-            if ((err = launch_plan(A, st)) != cudaSuccess) return fail_cuda(e, err, res);
+            if ((err = launch_plan(dA, st)) != cudaSuccess) return fail_cuda(e, err, res);
             ++launches;
             cudaMemcpyAsync(hl, dlev, sizeof(DevLevel), cudaMemcpyDeviceToHost, st);
             cudaMemcpyAsync(hc, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
@@ -635,31 +663,42 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
             cudaEventRecord(e->ev_a, st);
             DevCtl *dctl = (DevCtl *)e->ctl.p;
             if (per_block) {
-                // one launch per block in the reference's order, each after a snapshot
+                // one launch per block in the reference's order, each after a snapshot; the
+                // block's items are its window of the level kernel's item space (a unary block
+                // is copied into ublocks[0], items [0, its items))
+                long long base[7];
+                base[OP_NEG] = base[OP_X] = base[OP_F] = base[OP_G] = 0;
+                base[OP_AND] = hl->win_hi[1];
+                base[OP_OR] = hl->win_hi[1] + hl->total_items[OP_AND];
+                base[OP_U] = hl->win_hi[1] + hl->win_hi[2];
                 size_t nb_level = 0;
-                long long base = 0;
                 for (int op = 0; op < 7; ++op) {
+                    const bool un = op == OP_NEG || op == OP_X || op == OP_F || op == OP_G;
                     for (int k = 0; k < hl->nblocks[op]; ++k) {
                         const BlockDesc &B = hl->blocks[op][k];
                         cudaMemcpyAsync((DevCtl *)e->snaps.p + nb_level, e->ctl.p, sizeof(DevCtl),
                                         cudaMemcpyDeviceToDevice, st);
-                        long long *win = (long long *)e->h_win.p + 2 * nb_level;
-                        win[0] = base + B.item0;
-                        win[1] = base + B.item0 + B.items;
+                        long long *win = (long long *)e->h_win.p + 8 * nb_level;
+                        const long long lo = un ? 0 : base[op] + B.item0, hi = lo + B.items;
+                        win[0] = lo;  // queue[0]
+                        win[1] = hi;  // win_hi[0]
+                        if (un)  // the level kernel's unary items come from ublocks: this block alone
+                            cudaMemcpyAsync(&dlev->ublocks[0], &dlev->blocks[op][k], sizeof(BlockDesc),
+                                            cudaMemcpyDeviceToDevice, st);
                         cudaMemcpyAsync(&dctl->queue[0], &win[0], sizeof(u64), cudaMemcpyHostToDevice, st);
-                        cudaMemcpyAsync(&dlev->item_hi_all, &win[1], sizeof(long long), cudaMemcpyHostToDevice, st);
+                        cudaMemcpyAsync(&dlev->win_hi[0], &win[1], sizeof(long long), cudaMemcpyHostToDevice, st);
                         const int grid = (int)std::min<long long>(B.items, max_grid);
-                        if ((err = launch_level(A, grid, block_threads, st)) != cudaSuccess)
+                        if ((err = launch_level(A, dA, grid, block_threads, st)) != cudaSuccess)
                             return fail_cuda(e, err, res);
                         ++launches;
                         ++nb_level;
                     }
-                    base += hl->total_items[op];
                 }
             } else {
-                const int grid = (int)std::min<long long>(hl->item_hi_all, max_grid);
-                if (grid > 0) {
-                    if ((err = launch_level(A, grid, block_threads, st)) != cudaSuccess) return fail_cuda(e, err, res);
+                if (hl->win_hi[0] > 0) {
+                    const int grid = (int)std::min<long long>(hl->win_hi[0], max_grid);
+                    if ((err = launch_level(A, dA, grid, block_threads, st)) != cudaSuccess)
+                        return fail_cuda(e, err, res);
                     ++launches;
                 }
             }

@@ -18,6 +18,8 @@
 //   relaxed keys ....... :57-141 (KEY_REF, types 1/2/3 and the exact 126-bit pack)
 //   found .............. :243 (atomicCAS on a found word)
 // Every device wait is bounded; giving up sets a status bit the host reads.
+#include <atomic>
+
 #include "ltl_kernels.cuh"
 
 namespace ltlg {
@@ -32,7 +34,6 @@ constexpr u32 FIELD_OVERFLOW = 0xFFFFFFFEu;
 constexpr unsigned FULL = 0xFFFFFFFFu;
 constexpr long long WAIT_SPINS = 1ll << 22;    // slot publication wait (with nanosleep): ~1 s
 constexpr long long MBAR_SPINS = 1ll << 24;    // bulk-copy completion wait
-constexpr int UNARY_GROUP = 4;                 // source rows a warp evaluates together
 
 // MurmurHash3's 64-bit finaliser (Appleby, public domain).
 __device__ __forceinline__ u64 fmix64(u64 x) {
@@ -70,19 +71,25 @@ __device__ __forceinline__ u64 until_bits(u64 x, u64 y) {
     return until_rev(xr | yr, yr);
 }
 
+// Operator classes: each kernel runs one class; within the unary class (~ X F G) and the
+// and/or class the operator is a warp-uniform runtime value.
+constexpr int OP_ANDOR = 8, OP_UNARY = 9;
+
 template <int OP>
-__device__ __forceinline__ u64 uop(u64 w, u64 meta) {
+__device__ __forceinline__ u64 uop(u64 w, u64 meta, int rop) {
+    const int op = OP == OP_UNARY ? rop : OP;
     const u64 m = meta & LENMASK;
-    if (OP == OP_NEG) return ~w & m;
-    if (OP == OP_X) return w >> 1;
-    if (OP == OP_F) return fin_bits(w);
+    if (op == OP_NEG) return ~w & m;
+    if (op == OP_X) return w >> 1;
+    if (op == OP_F) return fin_bits(w);
     return glob_bits(w, m);  // OP_G
 }
 
 template <int OP>
-__device__ __forceinline__ u64 bop(u64 a, u64 b) {
-    if (OP == OP_AND) return a & b;
-    if (OP == OP_OR) return a | b;
+__device__ __forceinline__ u64 bop(u64 a, u64 b, int rop) {
+    const int op = OP == OP_ANDOR ? rop : OP;
+    if (op == OP_AND) return a & b;
+    if (op == OP_OR) return a | b;
     return until_bits(a, b);
 }
 
@@ -180,6 +187,7 @@ struct BinGen {
     const ulonglong2 *left;   // shared-memory tile, row stride nch
     const ulonglong2 *right;  // global right row
     int nch;
+    int rop;
     __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldg(right + c); }
     __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 r) const {
         if (OP == OP_U) {
@@ -189,7 +197,7 @@ struct BinGen {
             return make_ulonglong2(until_rev(lx | rx, rx), until_rev(ly | ry, ry));
         }
         const ulonglong2 l = left[t * nch + c];
-        return make_ulonglong2(bop<OP>(l.x, r.x), bop<OP>(l.y, r.y));
+        return make_ulonglong2(bop<OP>(l.x, r.x, rop), bop<OP>(l.y, r.y, rop));
     }
 };
 
@@ -198,10 +206,11 @@ struct UnGen {
     const u64 *src0;  // first source row of the group; rows are consecutive
     const ulonglong2 *meta;
     int pitch;
+    int rop;
     __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldg(meta + c); }
     __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 m) const {
         const ulonglong2 s = __ldg(reinterpret_cast<const ulonglong2 *>(src0 + (size_t)t * pitch) + c);
-        return make_ulonglong2(uop<OP>(s.x, m.x), uop<OP>(s.y, m.y));
+        return make_ulonglong2(uop<OP>(s.x, m.x, rop), uop<OP>(s.y, m.y, rop));
     }
 };
 
@@ -430,11 +439,10 @@ __device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u
 
 // Fingerprints, acceptance, found flag, uniqueness for NC candidates of one warp.
 template <int NC, class Gen, class ParentOf>
-__device__ __forceinline__ void finish(const LevelArgs &A, const Gen &g, u64 (&h)[NC], u32 bad, int cnt,
+__device__ __forceinline__ void finish(const LevelArgs &A, const Gen &g, u64 (&h)[NC], u32 bad, u32 valid,
                                        ParentOf parent_of, int lane) {
     const u64 sum = reduce_to_lane<NC>(h, lane);
     const u32 anybad = __reduce_or_sync(FULL, bad);
-    const u32 valid = cnt >= 32 ? FULL : ((1u << cnt) - 1u);
     const u32 acc = ~anybad & valid;
     const u64 myparent = parent_of(lane);
     if (acc) {
@@ -448,7 +456,8 @@ __device__ __forceinline__ void finish(const LevelArgs &A, const Gen &g, u64 (&h
     if (A.key_mode == KEY_HASH64) {
         kh = fp;
     } else if (A.key_mode == KEY_REF) {
-        for (int t = 0; t < cnt; ++t) {
+        for (int t = 0; t < NC; ++t) {
+            if (!((valid >> t) & 1u)) continue;
             u64 a, b;
             ref_key(A, g, t, lane, a, b);
             if (lane == t) {
@@ -458,7 +467,7 @@ __device__ __forceinline__ void finish(const LevelArgs &A, const Gen &g, u64 (&h
         }
         fp = fmix64(kh ^ fmix64(kl + 0x5ad0dedull));
     }
-    resolve<NC>(A, g, fp, lane < cnt, myparent, kh, kl, lane);
+    resolve<NC>(A, g, fp, (valid >> lane) & 1u, myparent, kh, kl, lane);
 }
 
 __device__ __forceinline__ bool found_stop(const LevelArgs &A) {
@@ -466,61 +475,82 @@ __device__ __forceinline__ bool found_stop(const LevelArgs &A) {
 }
 
 // ---------------------------------------------------------------- work items
-// Each operator path is compiled as its own function so registers are allocated per path.
-template <int OP, int HK>
-__device__ __noinline__ void unary_item(const LevelArgs &A, const BlockDesc &B, long long local, int warp, int nwarps, int lane,
-                           u64 &evals) {
-    const long long s_first = B.r0 + local * A.unary_rows;
-    const long long s_end = min(B.r1, s_first + (long long)A.unary_rows);
+// Operator of slot j of a fused unary block: 0 ~, 1 X, 2 F, 3 G.
+__device__ __forceinline__ int unary_slot_op(int j) { return j == 0 ? OP_NEG : j == 1 ? OP_X : j == 2 ? OP_F : OP_G; }
+
+// Candidate t of a fused unary item: source row t >> 2, operator slot t & 3.
+struct FusedUnGen {
+    const u64 *src0;  // first source row of the item; rows are consecutive
+    const ulonglong2 *meta;
+    int pitch;
+    __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldg(meta + c); }
+    __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 m) const {
+        const ulonglong2 s = __ldg(reinterpret_cast<const ulonglong2 *>(src0 + (size_t)(t >> 2) * pitch) + c);
+        const int op = unary_slot_op(t & 3);
+        return make_ulonglong2(uop<OP_UNARY>(s.x, m.x, op), uop<OP_UNARY>(s.y, m.y, op));
+    }
+};
+
+// One warp evaluates every operator of `mask` on source rows [s, s + rows) (rows <=
+// UNARY_ROWS): each source chunk is loaded once for all of them.
+template <int HK>
+__device__ __forceinline__ void unary_fused(const LevelArgs &A, int mask, long long s, int rows, int lane,
+                                            u64 &evals) {
+    constexpr int NC = 4 * UNARY_ROWS;
     const int nch = A.pitch >> 1;
     const ulonglong2 *meta = reinterpret_cast<const ulonglong2 *>(A.wmeta);
-    for (long long s = s_first + (long long)warp * UNARY_GROUP; s < s_end; s += (long long)nwarps * UNARY_GROUP) {
-        if (__any_sync(FULL, found_stop(A))) return;  // warp-uniform: lanes must not split
-        const int cnt = (int)min((long long)UNARY_GROUP, s_end - s);
-        const u64 *src0 = A.cache + (u64)s * A.pitch;
-        u64 h[UNARY_GROUP];
+    const u64 *src0 = A.cache + (u64)s * A.pitch;
+    u64 h[NC];
 #pragma unroll
-        for (int t = 0; t < UNARY_GROUP; ++t) h[t] = 0;
-        u32 bad = 0;
-        for (int c0 = lane; c0 < nch; c0 += 64) {
-            ulonglong2 sv[2][UNARY_GROUP], mv[2];
+    for (int t = 0; t < NC; ++t) h[t] = 0;
+    u32 bad = 0;
+    for (int c0 = lane; c0 < nch; c0 += 64) {
+        ulonglong2 sv[2][UNARY_ROWS], mv[2];
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const int c = c0 + 32 * u;
-                if (c < nch) {
-                    mv[u] = __ldg(meta + c);
+        for (int u = 0; u < 2; ++u) {
+            const int c = c0 + 32 * u;
+            if (c < nch) {
+                mv[u] = __ldg(meta + c);
 #pragma unroll
-                    for (int t = 0; t < UNARY_GROUP; ++t)
-                        if (t < cnt) sv[u][t] = __ldg(reinterpret_cast<const ulonglong2 *>(src0 + (size_t)t * A.pitch) + c);
-                }
+                for (int r = 0; r < UNARY_ROWS; ++r)
+                    if (r < rows) sv[u][r] = __ldg(reinterpret_cast<const ulonglong2 *>(src0 + (size_t)r * A.pitch) + c);
             }
+        }
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const int c = c0 + 32 * u;
-                if (c < nch) {
-                    const u64 k = (2ull * (u64)c + 1ull) * WEYL;
-                    const bool v0 = 2 * c < A.n, v1 = 2 * c + 1 < A.n;
-                    const ulonglong2 m = mv[u];
+        for (int u = 0; u < 2; ++u) {
+            const int c = c0 + 32 * u;
+            if (c < nch) {
+                const u64 k = (2ull * (u64)c + 1ull) * WEYL;
+                const bool v0 = 2 * c < A.n, v1 = 2 * c + 1 < A.n;
+                const ulonglong2 m = mv[u];
 #pragma unroll
-                    for (int t = 0; t < UNARY_GROUP; ++t) {
-                        if (t < cnt) {
-                            const u64 w0 = uop<OP>(sv[u][t].x, m.x), w1 = uop<OP>(sv[u][t].y, m.y);
-                            h[t] += hw<HK>(w0, k, v0) + hw<HK>(w1, k + WEYL, v1);
-                            bad |= badbit(w0, w1, m.x, m.y) << t;
+                for (int r = 0; r < UNARY_ROWS; ++r) {
+                    if (r < rows) {
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            if ((mask >> j) & 1) {
+                                const int op = unary_slot_op(j);
+                                const u64 w0 = uop<OP_UNARY>(sv[u][r].x, m.x, op), w1 = uop<OP_UNARY>(sv[u][r].y, m.y, op);
+                                h[4 * r + j] += hw<HK>(w0, k, v0) + hw<HK>(w1, k + WEYL, v1);
+                                bad |= badbit(w0, w1, m.x, m.y) << (4 * r + j);
+                            }
                         }
                     }
                 }
             }
         }
-        UnGen<OP> g{src0, meta, A.pitch};
-        finish<UNARY_GROUP>(A, g, h, bad, cnt, [&](int t) { return pack_parent(OP, (u64)(s + t), 0); }, lane);
-        evals += (u64)cnt;
     }
+    u32 valid = 0;
+    for (int r = 0; r < rows; ++r) valid |= (u32)(mask & 15) << (4 * r);
+    FusedUnGen g{src0, meta, A.pitch};
+    finish<NC>(A, g, h, bad, valid,
+               [&](int t) { return pack_parent(unary_slot_op(t & 3), (u64)(s + (t >> 2)), 0); }, lane);
+    evals += (u64)__popc(valid);
 }
 
 template <int OP, int TL, int HK>
-__device__ void binary_row(const LevelArgs &A, const ulonglong2 *tile, int nl, long long l_first, long long r,
-                           int lane, u64 &evals) {
+__device__ void binary_row(const LevelArgs &A, int rop, const ulonglong2 *tile, int nl, long long l_first,
+                           long long r, int lane, u64 &evals) {
     constexpr int NC = OP == OP_U ? 2 * TL : TL;
     const int nch = A.pitch >> 1;
     const ulonglong2 *R = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)r * A.pitch);
@@ -560,7 +590,7 @@ __device__ void binary_row(const LevelArgs &A, const ulonglong2 *tile, int nl, l
                         h[2 * t + 1] += hw<HK>(b0, k, v0) + hw<HK>(b1, k + WEYL, v1);
                         bad |= (badbit(a0, a1, m.x, m.y) << (2 * t)) | (badbit(b0, b1, m.x, m.y) << (2 * t + 1));
                     } else {
-                        const u64 w0 = bop<OP>(lv.x, rv.x), w1 = bop<OP>(lv.y, rv.y);
+                        const u64 w0 = bop<OP>(lv.x, rv.x, rop), w1 = bop<OP>(lv.y, rv.y, rop);
                         h[t] += hw<HK>(w0, k, v0) + hw<HK>(w1, k + WEYL, v1);
                         bad |= badbit(w0, w1, m.x, m.y) << t;
                     }
@@ -569,22 +599,24 @@ __device__ void binary_row(const LevelArgs &A, const ulonglong2 *tile, int nl, l
         }
     }
     const int cnt = OP == OP_U ? 2 * nl : nl;
-    BinGen<OP> g{tile, R, nch};
-    finish<NC>(A, g, h, bad, cnt,
+    const u32 valid = cnt >= 32 ? FULL : ((1u << cnt) - 1u);
+    BinGen<OP> g{tile, R, nch, rop};
+    const int op = OP == OP_ANDOR ? rop : OP;
+    finish<NC>(A, g, h, bad, valid,
                [&](int t) {
                    if (OP == OP_U) {
                        const u64 l = (u64)(l_first + (t >> 1));
-                       return (t & 1) ? pack_parent(OP, (u64)r, l) : pack_parent(OP, l, (u64)r);
+                       return (t & 1) ? pack_parent(op, (u64)r, l) : pack_parent(op, l, (u64)r);
                    }
-                   return pack_parent(OP, (u64)(l_first + t), (u64)r);
+                   return pack_parent(op, (u64)(l_first + t), (u64)r);
                },
                lane);
     evals += (u64)cnt;
 }
 
 template <int OP, int TL, int HK>
-__device__ __noinline__ bool binary_item(const LevelArgs &A, const BlockDesc &B, long long local, u64 *tile, u64 *bar,
-                            u32 &phase, int warp, int nwarps, int lane, u64 &evals) {
+__device__ __noinline__ bool binary_item(const LevelArgs &A, int rop, const BlockDesc &B, long long local, u64 *tile,
+                                            u64 *bar, u32 &phase, unsigned *next_row, int lane, u64 &evals) {
     constexpr int TLOP = OP == OP_U ? TL / 2 : TL;  // U makes two candidates per pair
     const long long tl = local / B.tiles_r, tr = local % B.tiles_r;
     const long long l_first = B.l0 + tl * TLOP;
@@ -605,49 +637,95 @@ __device__ __noinline__ bool binary_item(const LevelArgs &A, const BlockDesc &B,
     }
     phase ^= 1u;
     const ulonglong2 *t2 = reinterpret_cast<const ulonglong2 *>(tile);
-    for (long long r = r_first + warp; r < r_end; r += nwarps) {
+    // warps take the item's right rows one at a time (less waiting at the item's end)
+    for (;;) {
+        long long r = 0;
+        if (lane == 0) r = r_first + (long long)atomicAdd(next_row, 1u);
+        r = __shfl_sync(FULL, r, 0);
+        if (r >= r_end) break;
         if (__any_sync(FULL, found_stop(A))) break;  // warp-uniform: lanes must not split
-        binary_row<OP, TLOP, HK>(A, t2, nl, l_first, r, lane, evals);
+        binary_row<OP, TLOP, HK>(A, rop, t2, nl, l_first, r, lane, evals);
     }
     return true;
 }
 
-// One level: every work item of every block of the plan in A.lev, drained through one
-// queue in the reference's operator order (~, &, |, X, F, G, U).
+// The unary part of a level: fused blocks (every unary operator over the same source rows),
+// items of A.unary_rows source rows; the CTA's warps take UNARY_ROWS rows at a time.
+template <int HK>
+__device__ __noinline__ void unary_item(const LevelArgs &A, const BlockDesc &B, long long local, int warp, int nwarps,
+                                        int lane, u64 &evals) {
+    const long long s_first = B.r0 + local * A.unary_rows;
+    const long long s_end = min(B.r1, s_first + (long long)A.unary_rows);
+    for (long long s = s_first + (long long)warp * UNARY_ROWS; s < s_end; s += (long long)nwarps * UNARY_ROWS) {
+        if (__any_sync(FULL, found_stop(A))) return;  // warp-uniform: lanes must not split
+        unary_fused<HK>(A, B.opmask, s, (int)min((long long)UNARY_ROWS, s_end - s), lane, evals);
+    }
+}
+
+__device__ __forceinline__ int find_block(const BlockDesc *blocks, int nb, long long in_op) {
+    int lo = 0, hi = nb - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (blocks[mid].item0 <= in_op)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Copy the arguments and the level's plan header into shared memory (thread 0).
+__device__ __forceinline__ void load_level(LevelArgs &A, const LevelArgs *A0) {
+    A = *A0;
+    const DevLevel *L = A.lev;
+    A.cost = L->cost;
+    A.check_only = L->check_only;
+    A.right_chunk = L->right_chunk;
+    A.unary_rows = L->unary_rows;
+}
+
+// One level: every work item of the plan in A.lev, drained through one queue
+// (ctl->queue[0] up to lev->win_hi[0]).  Item space: the fused unary blocks (win_hi[1]
+// items), then the & and | blocks (win_hi[2]), then the U blocks (win_hi[3]).  A binary item
+// stages a tile of left rows in shared memory with one bulk copy; the CTA's warps take the
+// item's right rows one at a time.
 template <int TL, int HK>
-__global__ void __launch_bounds__(256, 3) level_kernel(const __grid_constant__ LevelArgs A0) {
+__global__ void __launch_bounds__(256, 3) level_kernel(const LevelArgs *__restrict__ A0) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     u64 *tile = reinterpret_cast<u64 *>(smem_raw);
     __shared__ __align__(16) LevelArgs A;
     __shared__ __align__(8) u64 bar;
-    __shared__ long long s_item, s_hi, s_base[8];
-    __shared__ int s_halt, s_nblocks[8];
+    __shared__ long long s_item, s_hi, s_ub[5], s_cls[4], s_and;
+    __shared__ int s_halt, s_nub, s_nb[7];
+    __shared__ unsigned s_next_row;
     __shared__ u64 s_evals;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     if (threadIdx.x == 0) {
-        A = A0;
+        load_level(A, A0);
         const DevLevel *L = A.lev;
         s_halt = L->halt;
-        s_hi = L->item_hi_all;
+        s_hi = L->win_hi[0];
+        s_nub = L->nublocks;
         long long b = 0;
-        for (int op = 0; op < 7; ++op) {
-            s_base[op] = b;
-            s_nblocks[op] = L->nblocks[op];
-            b += L->total_items[op];
+        for (int k = 0; k < 4; ++k) {
+            s_ub[k] = b;
+            b += k < s_nub ? L->ublocks[k].items : 0;
         }
-        s_base[7] = b;
-        A.cost = L->cost;
-        A.check_only = L->check_only;
-        A.right_chunk = L->right_chunk;
-        A.unary_rows = L->unary_rows;
+        s_ub[4] = b;
+        s_cls[0] = 0;
+        s_cls[1] = L->win_hi[1];
+        s_cls[2] = s_cls[1] + L->win_hi[2];
+        s_cls[3] = s_cls[2] + L->win_hi[3];
+        s_and = L->total_items[OP_AND];
+        for (int op = 0; op < 7; ++op) s_nb[op] = L->nblocks[op];
         mbar_init(&bar, 1);
         fence_mbar_init();
         s_evals = 0;
     }
     __syncthreads();
     if (s_halt || s_hi <= 0) return;
-    u32 phase = 0;
     u64 evals = 0;
+    u32 phase = 0;
     for (;;) {
         if (threadIdx.x == 0) {
             long long it = -1;
@@ -656,36 +734,31 @@ __global__ void __launch_bounds__(256, 3) level_kernel(const __grid_constant__ L
                 if (it >= s_hi) it = -1;
             }
             s_item = it;
+            s_next_row = 0;
         }
         __syncthreads();
         const long long item = s_item;
         if (item < 0) break;
-        int op = 0;
-        while (op < 6 && item >= s_base[op + 1]) ++op;
-        const long long in_op = item - s_base[op];
-        const BlockDesc *blocks = A.lev->blocks[op];
-        int lo = 0, hi = s_nblocks[op] - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (blocks[mid].item0 <= in_op)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
-        const BlockDesc B = blocks[lo];
-        const long long local = in_op - B.item0;
         bool ok = true;
-        switch (op) {
-        case OP_NEG: unary_item<OP_NEG, HK>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_X: unary_item<OP_X, HK>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_F: unary_item<OP_F, HK>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_G: unary_item<OP_G, HK>(A, B, local, warp, nwarps, lane, evals); break;
-        case OP_AND: ok = binary_item<OP_AND, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
-        case OP_OR: ok = binary_item<OP_OR, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
-        default: ok = binary_item<OP_U, TL, HK>(A, B, local, tile, &bar, phase, warp, nwarps, lane, evals); break;
+        if (item < s_cls[1]) {
+            int k = 0;
+            while (k < s_nub - 1 && item >= s_ub[k + 1]) ++k;
+            unary_item<HK>(A, A.lev->ublocks[k], item - s_ub[k], warp, nwarps, lane, evals);
+        } else if (item < s_cls[2]) {
+            const long long in_cls = item - s_cls[1];
+            const int op = in_cls < s_and ? OP_AND : OP_OR;
+            const long long in_op = op == OP_AND ? in_cls : in_cls - s_and;
+            const BlockDesc *blocks = A.lev->blocks[op];
+            const BlockDesc B = blocks[find_block(blocks, s_nb[op], in_op)];
+            ok = binary_item<OP_ANDOR, TL, HK>(A, op, B, in_op - B.item0, tile, &bar, phase, &s_next_row, lane, evals);
+        } else {
+            const long long in_op = item - s_cls[2];
+            const BlockDesc *blocks = A.lev->blocks[OP_U];
+            const BlockDesc B = blocks[find_block(blocks, s_nb[OP_U], in_op)];
+            ok = binary_item<OP_U, TL, HK>(A, OP_U, B, in_op - B.item0, tile, &bar, phase, &s_next_row, lane, evals);
         }
         if (!ok) break;
-        __syncthreads();
+        __syncthreads();  // every warp is done with the tile before the next copy
     }
     if (lane == 0 && evals) atomicAdd(&s_evals, evals);
     __syncthreads();
@@ -695,8 +768,9 @@ __global__ void __launch_bounds__(256, 3) level_kernel(const __grid_constant__ L
 // The planner: one thread turns the level starts into the next level's plan, in the
 // reference's order (ltli6463.cu:1209-1440; NegType rule :1212): ~, & splits, | splits,
 // X, F, G, U splits; a split i pairs cost i with cost c - i - c_op, i = c1 .. (c - c_op)/2.
-__global__ void plan_kernel(const __grid_constant__ LevelArgs A) {
+__global__ void plan_kernel(const LevelArgs *__restrict__ pA) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const LevelArgs &A = *pA;
     DevLevel *L = A.lev;
     DevCtl *C = A.ctl;
     if (L->halt == 2) return;  // an over-long plan stops the rest of the graph
@@ -714,8 +788,9 @@ __global__ void plan_kernel(const __grid_constant__ LevelArgs A) {
         L->item_hi[k] = 0;
         C->queue[k] = 0;
     }
-    L->item_lo = 0;
     L->item_hi_all = 0;
+    L->nublocks = 0;
+    for (int k = 0; k < 4; ++k) L->win_hi[k] = 0;
     L->halt = halt ? 1 : 0;
     L->level_cands = 0;
     if (halt) return;
@@ -733,6 +808,8 @@ __global__ void plan_kernel(const __grid_constant__ LevelArgs A) {
         BlockDesc &b = L->blocks[op][k];
         b.op = op;
         b.lcost = lc;
+        b.opmask = op == OP_NEG ? 1 : op == OP_X ? 2 : op == OP_F ? 4 : op == OP_G ? 8 : 0;
+        b.pad = 0;
         b.l0 = l0;
         b.l1 = l1;
         b.r0 = r0;
@@ -769,12 +846,37 @@ __global__ void plan_kernel(const __grid_constant__ LevelArgs A) {
     // per warp so every SM takes part; a large level keeps the configured sizes.
     const bool small = (long long)cands < A.small_level;
     const int rc = small ? A.nwarps : A.right_chunk_big;
-    const int ur = small ? A.nwarps * UNARY_GROUP : A.unary_rows_big;
+    const int ur = small ? A.nwarps * UNARY_ROWS : A.unary_rows_big;
     L->right_chunk = rc;
     L->unary_rows = ur;
     L->check_only = L->on_the_fly;
     L->level_cands = cands;
     if (c < MAX_COSTS + 1) A.level_cands[c] = cands;
+    // Unary operators over the same source rows become one fused block.
+    L->nublocks = 0;
+    for (int j = 0; j < 4; ++j) {
+        const int op = unary_slot_op(j);
+        if (L->nblocks[op] == 0) continue;
+        const BlockDesc &b = L->blocks[op][0];
+        int u = 0;
+        while (u < L->nublocks && !(L->ublocks[u].r0 == b.r0 && L->ublocks[u].r1 == b.r1)) ++u;
+        if (u == L->nublocks) {
+            BlockDesc &f = L->ublocks[L->nublocks++];
+            f = b;
+            f.opmask = 0;
+            f.candidates = 0;
+        }
+        L->ublocks[u].opmask |= 1 << j;
+        L->ublocks[u].candidates += b.candidates;
+    }
+    for (int u = 0; u < L->nublocks; ++u) {
+        BlockDesc &f = L->ublocks[u];
+        f.item0 = L->win_hi[1];
+        f.items = (f.r1 - f.r0 + ur - 1) / ur;
+        f.tiles_r = 1;
+        L->win_hi[1] += f.items;
+        L->item_hi_all += f.items;
+    }
     for (int op = 0; op < 7; ++op) {
         long long items = 0;
         const bool bin = op == OP_AND || op == OP_OR || op == OP_U;
@@ -787,20 +889,25 @@ __global__ void plan_kernel(const __grid_constant__ LevelArgs A) {
                 b.items = ((b.l1 - b.l0 + tile - 1) / tile) * b.tiles_r;
             } else {
                 b.tiles_r = 1;
-                b.items = (b.r1 - b.r0 + ur - 1) / ur;
+                b.items = (b.r1 - b.r0 + ur - 1) / ur;  // items of this operator alone (per-block runs)
             }
             items += b.items;
         }
         L->total_items[op] = items;
         L->item_hi[op] = items;
-        L->item_hi_all += items;
+        if (bin) {
+            L->item_hi_all += items;
+            L->win_hi[op == OP_U ? 3 : 2] += items;
+        }
     }
+    L->win_hi[0] = L->item_hi_all;
 }
 
 // Letters: register rows [0, nalpha) in the hash set (duplicate letters stay rows,
 // as the reference stores every letter, ltli6463.cu:1134, :1189-1190).  One warp.
 template <int HK>
-__global__ void insert_letters_kernel(const __grid_constant__ LevelArgs A, int nalpha) {
+__global__ void insert_letters_kernel(const LevelArgs *__restrict__ pA, int nalpha) {
+    const LevelArgs &A = *pA;
     const int lane = threadIdx.x & 31;
     const int nch = A.pitch >> 1;
     const ulonglong2 *meta = reinterpret_cast<const ulonglong2 *>(A.wmeta);
@@ -919,12 +1026,12 @@ __global__ void apply_op_kernel(int op, const u64 *a, const u64 *b, const u64 *w
         const u64 m = wmeta[i];
         u64 w = 0, w2 = 0;
         switch (op) {
-        case OP_NEG: w = uop<OP_NEG>(x, m); break;
-        case OP_X: w = uop<OP_X>(x, m); break;
-        case OP_F: w = uop<OP_F>(x, m); break;
-        case OP_G: w = uop<OP_G>(x, m); break;
-        case OP_AND: w = bop<OP_AND>(x, y); break;
-        case OP_OR: w = bop<OP_OR>(x, y); break;
+        case OP_NEG: w = uop<OP_NEG>(x, m, OP_NEG); break;
+        case OP_X: w = uop<OP_X>(x, m, OP_X); break;
+        case OP_F: w = uop<OP_F>(x, m, OP_F); break;
+        case OP_G: w = uop<OP_G>(x, m, OP_G); break;
+        case OP_AND: w = bop<OP_AND>(x, y, OP_AND); break;
+        case OP_OR: w = bop<OP_OR>(x, y, OP_OR); break;
         case OP_U:
             w = until_bits(x, y);
             w2 = until_bits(y, x);
@@ -954,19 +1061,23 @@ int level_kernel_smem_bytes(int left_tile, int pitch) { return left_tile * pitch
 
 template <int TL, int HK>
 static cudaError_t smem_attr(int smem) {
-    static int attr_set = 48 * 1024;  // largest dynamic shared memory size enabled so far
-    if (smem <= attr_set) return cudaSuccess;
+    static std::atomic<int> attr_set{48 * 1024};  // largest dynamic shared memory size enabled so far
+    if (smem <= attr_set.load()) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(level_kernel<TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess) attr_set = smem;
+    if (e == cudaSuccess) {
+        int cur = attr_set.load();
+        while (cur < smem && !attr_set.compare_exchange_weak(cur, smem)) {
+        }
+    }
     return e;
 }
 
 template <int TL, int HK>
-static cudaError_t launch_tl(const LevelArgs &a, int grid, int block, cudaStream_t s) {
+static cudaError_t launch_tl(const LevelArgs &a, const LevelArgs *d, int grid, int block, cudaStream_t s) {
     const int smem = level_kernel_smem_bytes(TL, a.pitch);
     cudaError_t e = smem_attr<TL, HK>(smem);
     if (e != cudaSuccess) return e;
-    level_kernel<TL, HK><<<grid, block, smem, s>>>(a);
+    level_kernel<TL, HK><<<grid, block, smem, s>>>(d);
     return cudaGetLastError();
 }
 
@@ -978,9 +1089,10 @@ static int occupancy_tl(int block, int pitch) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<TL, HK>, block, smem) == cudaSuccess ? n : 0;
 }
 
-cudaError_t launch_level(const LevelArgs &a, int grid, int block, cudaStream_t s) {
-    if (a.hash_kind == 1) return a.left_tile == 4 ? launch_tl<4, 1>(a, grid, block, s) : launch_tl<8, 1>(a, grid, block, s);
-    return a.left_tile == 4 ? launch_tl<4, 0>(a, grid, block, s) : launch_tl<8, 0>(a, grid, block, s);
+cudaError_t launch_level(const LevelArgs &a, const LevelArgs *d, int grid, int block, cudaStream_t s) {
+    if (a.hash_kind == 1)
+        return a.left_tile == 4 ? launch_tl<4, 1>(a, d, grid, block, s) : launch_tl<8, 1>(a, d, grid, block, s);
+    return a.left_tile == 4 ? launch_tl<4, 0>(a, d, grid, block, s) : launch_tl<8, 0>(a, d, grid, block, s);
 }
 
 int level_kernel_max_ctas_per_sm(int left_tile, int hash_kind, int block, int pitch) {
@@ -988,16 +1100,16 @@ int level_kernel_max_ctas_per_sm(int left_tile, int hash_kind, int block, int pi
     return left_tile == 4 ? occupancy_tl<4, 0>(block, pitch) : occupancy_tl<8, 0>(block, pitch);
 }
 
-cudaError_t launch_plan(const LevelArgs &a, cudaStream_t s) {
-    plan_kernel<<<1, 32, 0, s>>>(a);
+cudaError_t launch_plan(const LevelArgs *d, cudaStream_t s) {
+    plan_kernel<<<1, 32, 0, s>>>(d);
     return cudaGetLastError();
 }
 
-cudaError_t launch_insert_letters(const LevelArgs &a, int nalpha, cudaStream_t s) {
+cudaError_t launch_insert_letters(const LevelArgs &a, const LevelArgs *d, int nalpha, cudaStream_t s) {
     if (a.hash_kind == 1)
-        insert_letters_kernel<1><<<1, 32, 0, s>>>(a, nalpha);
+        insert_letters_kernel<1><<<1, 32, 0, s>>>(d, nalpha);
     else
-        insert_letters_kernel<0><<<1, 32, 0, s>>>(a, nalpha);
+        insert_letters_kernel<0><<<1, 32, 0, s>>>(d, nalpha);
     return cudaGetLastError();
 }
 

@@ -45,6 +45,8 @@ struct DevCtl {
 struct BlockDesc {
     int op;
     int lcost;           // cost of the left operand (unary: of the operand)
+    int opmask;          // fused unary blocks: bit 0 ~, 1 X, 2 F, 3 G over the same source rows
+    int pad;
     long long l0, l1, r0, r1;
     long long item0;     // first work item of this block within its operator
     long long items;     // work items of this block
@@ -53,6 +55,7 @@ struct BlockDesc {
 };
 
 constexpr int MAX_SPLITS = 64;   // blocks per operator and level in a device-planned level
+constexpr int UNARY_ROWS = 2;    // source rows per unary work item (each with every operator of its mask)
 constexpr int MAX_COSTS = 512;   // level starts kept on the device
 
 // The plan of the level being enumerated, in device memory.  The planner kernel writes it
@@ -62,14 +65,18 @@ struct DevLevel {
     int halt;            // 1: every operator kernel of this level exits at once
     int check_only;      // on-the-fly: acceptance only, no dedupe, no storing
     int on_the_fly;      // set by the host: plan check-only levels and ignore the overflow bit
-    long long item_lo;   // the level kernel takes items from ctl->queue[0] in [item_lo, item_hi_all)
-    long long item_hi_all;
+    long long item_hi_all;  // all work items of the level
+    long long win_hi[4];    // [0]: the level kernel takes items from ctl->queue[0] below it; [1..3]: items of
+                            // the fused unary blocks, of the & and | blocks, of the U blocks
     int right_chunk;
     int unary_rows;
     int nblocks[8];
     long long total_items[8];
     long long item_hi[8];  // an operator kernel takes items from its queue until item_hi
     u64 level_cands;     // candidates of the level, counted as the reference counts them
+    int nublocks;        // fused unary blocks: the unary kernel works from these
+    int pad2;
+    BlockDesc ublocks[4];
     BlockDesc blocks[7][MAX_SPLITS];
 };
 
@@ -110,13 +117,15 @@ struct LevelArgs {
     int unary_rows;
 };
 
-// Launch wrappers (ltl_kernels.cu).  The level kernel drains the work items of every block
-// of the planned level; binary items stage left tiles of left_tile rows (U: half).
+// Launch wrappers (ltl_kernels.cu).  A level is one kernel (launch_level) that drains
+// ctl->queue[0]; the planner (launch_plan) writes its plan first.  The kernels read their
+// arguments from `d`, a copy of `a` in device memory, so a captured graph stays valid while
+// `*d` changes; `a` (host) selects the template instance and the shared-memory size.
 int level_kernel_smem_bytes(int left_tile, int pitch);
 int level_kernel_max_ctas_per_sm(int left_tile, int hash_kind, int block, int pitch);
-cudaError_t launch_level(const LevelArgs &a, int grid, int block, cudaStream_t s);
-cudaError_t launch_plan(const LevelArgs &a, cudaStream_t s);
-cudaError_t launch_insert_letters(const LevelArgs &a, int nalpha, cudaStream_t s);
+cudaError_t launch_level(const LevelArgs &a, const LevelArgs *d, int grid, int block, cudaStream_t s);
+cudaError_t launch_plan(const LevelArgs *d, cudaStream_t s);
+cudaError_t launch_insert_letters(const LevelArgs &a, const LevelArgs *d, int nalpha, cudaStream_t s);
 cudaError_t launch_walk(const u64 *parents, int nalpha, u64 found, u64 *out, int cap, cudaStream_t s);
 cudaError_t launch_apply_op(int op, const u64 *a, const u64 *b, const u64 *wmeta, int n, int pitch, int count,
                             u64 *out, u64 *out2, u64 *fp, cudaStream_t s);

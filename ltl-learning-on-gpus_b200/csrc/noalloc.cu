@@ -196,6 +196,7 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     };
     DevCtl *ctl = (DevCtl *)carve(sizeof(DevCtl));
     DevLevel *lev = (DevLevel *)carve(sizeof(DevLevel));
+    LevelArgs *dargs = (LevelArgs *)carve(sizeof(LevelArgs));
     long long *ls = (long long *)carve((MAX_COSTS + 2) * sizeof(long long));
     u64 *lcands = (u64 *)carve((MAX_COSTS + 2) * sizeof(u64));
     u64 *wmeta = (u64 *)carve((size_t)pitch * 8);
@@ -224,7 +225,7 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     DevCtl hc;
     memset(&hc, 0, sizeof(hc));
     hc.row_count = (u64)nalpha;
-    int lev_head[6] = {c1, 0, 0, 0, 0, 0};  // cost, halt, check_only, on_the_fly, right_chunk, unary_rows
+    int lev_head[4] = {c1, 0, 0, 0};  // cost, halt, check_only, on_the_fly
     if ((err = cudaMemcpy(cache, letters, (size_t)nalpha * pitch * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (err = cudaMemcpy(wmeta, wm, (size_t)pitch * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (err = cudaMemset(kmeta, 0, (size_t)pitch * 4)) != cudaSuccess ||
@@ -273,13 +274,14 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     A.lev = lev;
     A.ls = ls;
     A.level_cands = lcands;
-    if ((err = launch_insert_letters(A, nalpha, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
+    if ((err = cudaMemcpy(dargs, &A, sizeof(A), cudaMemcpyHostToDevice)) != cudaSuccess) return LTLG_CUDA_ERROR;
+    if ((err = launch_insert_letters(A, dargs, nalpha, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
 
     // Levels: planner, level kernel, then read the control record.
     int last_cost = c1;
     for (;;) {
-        if ((err = launch_plan(A, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
-        if ((err = launch_level(A, (int)max_grid, block_threads, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
+        if ((err = launch_plan(dargs, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
+        if ((err = launch_level(A, dargs, (int)max_grid, block_threads, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
         int head[2];
         if ((err = cudaMemcpy(&hc, ctl, sizeof(hc), cudaMemcpyDeviceToHost)) != cudaSuccess ||
             (err = cudaMemcpy(head, lev, sizeof(head), cudaMemcpyDeviceToHost)) != cudaSuccess)

@@ -227,7 +227,7 @@ def run_ours(a):
     opts = dict(neg_type=1, max_cost=a.max_cost, stop_at_found=not a.no_stop)
 
     def seq_step():
-        return [eng.learn(inst, **opts) for inst in batch]
+        return [eng.learn(inst, record_levels=True, **opts) for inst in batch]
 
     def batch_step():
         return pool.learn(batch, **opts) if pool else seq_step()
@@ -245,6 +245,7 @@ def run_ours(a):
 
     step_ms, kern_ms, launches = [], [], 0
     uniq_e2e = cand_e2e = uniq_seq = cand_seq = 0
+    level_launches = 0  # level-kernel launches of the one-at-a-time pass
     ttm, costs = [], []
     h2d = d2h = 0
     with Clocks(local, enabled=not a.no_clocks) as clk:
@@ -276,6 +277,7 @@ def run_ours(a):
             for inst, r in zip(batch, seq):
                 uniq_seq += r.rows - len(inst.alphabet)
                 cand_seq += r.evaluated - len(inst.alphabet)
+                level_launches += len(r.levels)
     clocks = clk.summary()
     K = a.steps
     step_t = sum(step_ms) / 1e3
@@ -296,6 +298,7 @@ def run_ours(a):
         alg_bytes = (cand_seq + uniq_seq) * per_unit  # this rank's bytes over its own kernel time
         achieved = alg_bytes / (sum(kern_ms) / 1e3) / 1e9
         tpc = profile_traffic_per_candidate()
+        nl = max(1, level_launches)
         line = {
             "metric": METRIC, "value": tot[2] / kern_t, "unit": UNIT, "n_gpus": ws, "steps": K,
             "warmup": a.warmup, "ms_per_step": 1e3 * step_t / K, "higher_is_better": True, "scaling": "weak",
@@ -313,9 +316,14 @@ def run_ours(a):
                     "d2h_bytes_per_step": d2h // K, "candidate_cs_per_s": tot[1] / step_t},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": (tpc * cand_seq / max(1, K * len(batch))) if tpc else None,
+                         "traffic": (tpc * cand_seq / nl) if tpc else None,
+                         "alg_bytes_per_launch": alg_bytes / nl,
                          "kernel": "level_kernel", "bytes_per_unit": per_unit,
-                         "units": "candidates evaluated + uniques stored"},
+                         "units": "candidates evaluated + uniques stored",
+                         "timing": "level time from CUDA events on the engine stream (planner + level kernel "
+                                   "+ 2 small D2H copies per level), summed over the one-at-a-time pass",
+                         "traffic_source": "ncu DRAM bytes per candidate of the cost-8 level_kernel launch "
+                                           "(profiles/level_kernel_cfg2.txt) x mean candidates per launch"},
             "gpu_launches": launches,
             "clocks": clocks,
         }

@@ -211,24 +211,36 @@ def generate_hamming(seed: int, nprops: int, npos: int, nneg: int, lmin: int, lm
             continue
         seen = {(ln, b[:ln].tobytes()) for ln, b in zip(pos_l, pos_b)}
         neg_l, neg_b = [], []
-        tries = 0
-        while len(neg_l) < nneg and tries < 200 * nneg:
-            tries += 1
-            src = int(rng.integers(npos))
-            ln = pos_l[src]
-            b = pos_b[src].copy()
-            for _k in range(int(rng.integers(flips[0], flips[1] + 1))):
-                b[int(rng.integers(ln)), int(rng.integers(nprops))] ^= True
-            key = (ln, b[:ln].tobytes())
-            if key in seen:
-                continue
-            w = np.array([[int(sum(int(b[k, j]) << k for k in range(ln)))] for j in range(nprops)],
-                         dtype=np.uint64)
-            m = np.array([(1 << ln) - 1], dtype=np.uint64)
-            if int(eval_cs(f, w, m)[0]) & 1:
-                continue
-            seen.add(key)
-            neg_l.append(ln); neg_b.append(b)
+        plen = np.asarray(pos_l, dtype=np.int64)
+        pbits = np.stack(pos_b)
+        weights = (_ONE << np.arange(lmax, dtype=np.uint64))
+        for _round in range(200):
+            if len(neg_l) >= nneg:
+                break
+            # a batch of flipped copies, evaluated together; kept in draw order
+            src = rng.integers(npos, size=batch)
+            lens = plen[src]
+            bits = pbits[src].copy()
+            nfl = rng.integers(flips[0], flips[1] + 1, size=batch)
+            rows = np.arange(batch)
+            for k in range(flips[1]):
+                at = (rng.random(batch) * lens).astype(np.int64)
+                prop = rng.integers(nprops, size=batch)
+                act = nfl > k
+                bits[rows[act], at[act], prop[act]] ^= True
+            atoms = np.stack([(bits[:, :, j].astype(np.uint64) * weights).sum(axis=1, dtype=np.uint64)
+                              for j in range(nprops)])
+            mask = (_ONE << lens.astype(np.uint64)) - _ONE
+            false_ = (eval_cs(f, atoms, mask) & _ONE) == 0
+            for i in np.nonzero(false_)[0]:
+                ln = int(lens[i])
+                key = (ln, bits[i, :ln].tobytes())
+                if key in seen:
+                    continue
+                seen.add(key)
+                neg_l.append(ln); neg_b.append(bits[i])
+                if len(neg_l) == nneg:
+                    break
         if len(neg_l) == nneg:
             steps, offsets = _pack(letters, pos_l + neg_l, pos_b + neg_b)
             return Instance(npos, len(neg_l), letters, steps, offsets, formula_str(f, letters))

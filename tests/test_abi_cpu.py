@@ -64,3 +64,18 @@ def test_generator_is_deterministic():
     # every negative differs from every positive
     lines = h.trace_lines()
     assert not set(lines[:40]) & set(lines[40:])
+
+
+def test_hamming_negatives_are_near_misses():
+    """Each negative is a positive with 1-3 bits flipped, falsifies the hidden formula, and
+    repeats no positive."""
+    h = gen.generate_hamming(7, 4, 60, 60, 20, 48, 0.5, 6)
+    offs, steps = h.offsets, h.steps
+    tr = [steps[offs[i]:offs[i + 1]] for i in range(h.n)]
+    pos, neg = tr[:60], tr[60:]
+    for t in neg:
+        best = min((sum(bin(int(a) ^ int(b)).count("1") for a, b in zip(t, p)) for p in pos if len(p) == len(t)),
+                   default=None)
+        assert best is not None and 1 <= best <= 3
+    cs = h.atom_cs()
+    assert cs.shape[0] == 4

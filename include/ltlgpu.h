@@ -208,6 +208,67 @@ LTLG_API int ltlg_device_apply_op(int32_t op, const uint64_t *a, const uint64_t 
 LTLG_API int ltlg_read_scarlet(const char *path, ltlg_traces *out);
 LTLG_API void ltlg_traces_free(ltlg_traces *t);
 
+/* ---- Learned block order (no counterpart in the reference: its enumerator always runs a
+ * level's blocks in the fixed operator / split order).  A scorer, a multilayer perceptron
+ * 32 -> 64 -> 64 -> 1 (ReLU; BF16 operands, FP32 accumulation), rates each (operator, left
+ * cost, right cost) block of a level; with ltlg_options.order = LTLG_ORDER_LEARNED the level's
+ * blocks are drained highest score first.  Only the order changes: the level still runs to its
+ * end unless a find stops it, so the cost found is the plain enumerator's. */
+#define LTLG_SCORER_FEATURES 32
+#define LTLG_SCORER_PARAMS 6337  /* W1[64][32], b1[64], W2[64][64], b2[64], W3[64], b3 (FP32) */
+
+typedef struct ltlg_block_record {
+    int32_t cost;              /* the level */
+    int32_t op;                /* operator code */
+    int32_t lcost, rcost;      /* operand costs (rcost 0 for unary blocks) */
+    int32_t position;          /* index in the reference's order within the level */
+    int32_t won;               /* 1: the block holds a candidate that accepts */
+    int64_t candidates;
+    float features[LTLG_SCORER_FEATURES];
+} ltlg_block_record;
+
+/* What a block's features are computed from (host side; the device planner uses the same
+ * function).  Costs are level costs, rows are cache rows, "c_" counts are candidates. */
+typedef struct ltlg_block_info {
+    int32_t op, cost, c1, lcost, rcost, position, nblocks, pad_;
+    int64_t lrows, rrows, candidates, level_cands;
+    int64_t u_left, u_right, c_left, c_right, u_prev, c_prev;
+    int32_t npos, nneg, nalpha, pad2_;
+} ltlg_block_info;
+
+LTLG_API void ltlg_block_features(const ltlg_block_info *info, float *features);
+
+/* Load a scorer (LTLG_SCORER_PARAMS floats) into the engine / every engine of a batch. */
+LTLG_API int ltlg_engine_set_scorer(ltlg_engine *eng, const float *params, int32_t count);
+LTLG_API int ltlg_batch_set_scorer(ltlg_batch *b, const float *params, int32_t count);
+
+/* Training records of one instance: learn it in plain order (stop at the first find), then run
+ * every block of the level of the find again, alone, in check-only mode (acceptance tested on
+ * every candidate, nothing stored) and record whether it holds an accepting candidate.  Writes
+ * up to cap records and their count; res is the learn's result (free with ltlg_result_free). */
+LTLG_API int ltlg_engine_label_blocks(ltlg_engine *eng, const ltlg_traces *traces, const ltlg_options *opt,
+                                      ltlg_block_record *records, int32_t cap, int32_t *count, ltlg_result *res);
+
+/* The scorer's kernels on host arrays (features: count x 32 floats, row-major).
+ * forward: logits.  grad: gradient of the mean weighted binary cross-entropy (weight pos_weight
+ * on label-1 records) and the loss.  train: Adam on the GPU, params updated in place; epoch_loss
+ * (optional) receives the mean loss of each epoch. */
+typedef struct ltlg_train_config {
+    int32_t epochs;
+    int32_t batch;
+    float lr;
+    float pos_weight;
+    float beta1, beta2, eps;
+    float weight_decay;
+    uint64_t seed;             /* shuffling */
+} ltlg_train_config;
+
+LTLG_API int ltlg_scorer_forward(const float *params, const float *features, int32_t count, float *logits);
+LTLG_API int ltlg_scorer_grad(const float *params, const float *features, const float *labels, int32_t count,
+                              float pos_weight, float *grad, float *loss);
+LTLG_API int ltlg_scorer_train(float *params, const float *features, const float *labels, int32_t count,
+                               const ltlg_train_config *cfg, float *epoch_loss);
+
 LTLG_API const char *ltlg_status_string(int status);
 LTLG_API int ltlg_abi_version(void);
 

@@ -29,8 +29,12 @@ EXPORTED = [
     "ltlg_engine_create", "ltlg_engine_destroy", "ltlg_engine_learn", "ltlg_learn", "ltlg_result_free",
     "ltlg_engine_read_rows", "ltlg_engine_level_starts", "ltlg_device_apply_op", "ltlg_read_scarlet",
     "ltlg_traces_free", "ltlg_engine_stream", "ltlg_batch_create", "ltlg_batch_destroy", "ltlg_batch_learn",
-    "ltlg_batch_stream", "ltlg_learn_noalloc",
+    "ltlg_batch_stream", "ltlg_learn_noalloc", "ltlg_block_features", "ltlg_engine_set_scorer",
+    "ltlg_batch_set_scorer", "ltlg_engine_label_blocks", "ltlg_scorer_forward", "ltlg_scorer_grad",
+    "ltlg_scorer_train",
 ]
+SCORER_FEATURES = 32
+SCORER_PARAMS = 6337
 
 
 class Traces(C.Structure):
@@ -70,6 +74,27 @@ class Result(C.Structure):
                 ("on_the_fly", C.c_int32), ("launches", C.c_int32)]
 
 
+class BlockInfo(C.Structure):
+    _fields_ = [("op", C.c_int32), ("cost", C.c_int32), ("c1", C.c_int32), ("lcost", C.c_int32),
+                ("rcost", C.c_int32), ("position", C.c_int32), ("nblocks", C.c_int32), ("pad_", C.c_int32),
+                ("lrows", C.c_int64), ("rrows", C.c_int64), ("candidates", C.c_int64), ("level_cands", C.c_int64),
+                ("u_left", C.c_int64), ("u_right", C.c_int64), ("c_left", C.c_int64), ("c_right", C.c_int64),
+                ("u_prev", C.c_int64), ("c_prev", C.c_int64), ("npos", C.c_int32), ("nneg", C.c_int32),
+                ("nalpha", C.c_int32), ("pad2_", C.c_int32)]
+
+
+class BlockRecord(C.Structure):
+    _fields_ = [("cost", C.c_int32), ("op", C.c_int32), ("lcost", C.c_int32), ("rcost", C.c_int32),
+                ("position", C.c_int32), ("won", C.c_int32), ("candidates", C.c_int64),
+                ("features", C.c_float * SCORER_FEATURES)]
+
+
+class TrainConfig(C.Structure):
+    _fields_ = [("epochs", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float), ("pos_weight", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float), ("weight_decay", C.c_float),
+                ("seed", C.c_uint64)]
+
+
 _lib = None
 
 
@@ -104,6 +129,17 @@ def lib():
                                        C.POINTER(Result)]
         L.ltlg_batch_stream.argtypes = [C.c_void_p, C.c_int32]
         L.ltlg_batch_stream.restype = C.c_void_p
+        fp = C.POINTER(C.c_float)
+        L.ltlg_block_features.argtypes = [C.POINTER(BlockInfo), fp]
+        L.ltlg_block_features.restype = None
+        L.ltlg_engine_set_scorer.argtypes = [C.c_void_p, fp, C.c_int32]
+        L.ltlg_batch_set_scorer.argtypes = [C.c_void_p, fp, C.c_int32]
+        L.ltlg_engine_label_blocks.argtypes = [C.c_void_p, C.POINTER(Traces), C.POINTER(Options),
+                                               C.POINTER(BlockRecord), C.c_int32, C.POINTER(C.c_int32),
+                                               C.POINTER(Result)]
+        L.ltlg_scorer_forward.argtypes = [fp, fp, C.c_int32, fp]
+        L.ltlg_scorer_grad.argtypes = [fp, fp, fp, C.c_int32, C.c_float, fp, fp]
+        L.ltlg_scorer_train.argtypes = [fp, fp, fp, C.c_int32, C.POINTER(TrainConfig), fp]
         _lib = L
     return _lib
 
@@ -231,6 +267,40 @@ class Engine:
         """The engine's cudaStream_t as an integer handle."""
         return lib().ltlg_engine_stream(self._h) or 0
 
+    def set_scorer(self, params: np.ndarray):
+        """Load the block-order scorer (SCORER_PARAMS floats) for order=ORDER_LEARNED."""
+        p = _f32(params, SCORER_PARAMS)
+        rc = lib().ltlg_engine_set_scorer(self._h, _fp(p), SCORER_PARAMS)
+        if rc != 0:
+            raise RuntimeError(f"set_scorer failed: {status_string(rc)}")
+
+    def label_blocks(self, inst: Instance, cap: int = 4096, **kw):
+        """Learn in plain order, then label every block of the level of the find (holds an
+        accepting candidate or not).  Returns (LearnResult, records: list of dicts,
+        features: float32 [k, 32], won: int32 [k])."""
+        o = make_options(**kw)
+        t, keep = _traces(inst)
+        recs = (BlockRecord * cap)()
+        cnt = C.c_int32(0)
+        r = Result()
+        lib().ltlg_engine_label_blocks(self._h, C.byref(t), C.byref(o), recs, cap, C.byref(cnt), C.byref(r))
+        try:
+            out = _result(r)
+        finally:
+            lib().ltlg_result_free(C.byref(r))
+        self.n = inst.n
+        k = cnt.value
+        feats = np.zeros((k, SCORER_FEATURES), dtype=np.float32)
+        won = np.zeros(k, dtype=np.int32)
+        meta = []
+        for i in range(k):
+            x = recs[i]
+            feats[i] = np.frombuffer(x.features, dtype=np.float32, count=SCORER_FEATURES)
+            won[i] = x.won
+            meta.append(dict(cost=x.cost, op=OPS[x.op], lcost=x.lcost, rcost=x.rcost, position=x.position,
+                             candidates=x.candidates, won=x.won))
+        return out, meta, feats, won
+
     def level_starts(self, count: int) -> list:
         a = (C.c_int64 * count)()
         lib().ltlg_engine_level_starts(self._h, a, count)
@@ -287,6 +357,12 @@ class Batch:
     def stream(self, worker: int = 0) -> int:
         return lib().ltlg_batch_stream(self._h, worker) or 0
 
+    def set_scorer(self, params: np.ndarray):
+        p = _f32(params, SCORER_PARAMS)
+        rc = lib().ltlg_batch_set_scorer(self._h, _fp(p), SCORER_PARAMS)
+        if rc != 0:
+            raise RuntimeError(f"set_scorer failed: {status_string(rc)}")
+
     def learn(self, instances, **kw) -> list:
         o = make_options(**kw)
         n = len(instances)
@@ -317,6 +393,66 @@ def learn(inst: Instance, **kw) -> LearnResult:
         return _result(r)
     finally:
         lib().ltlg_result_free(C.byref(r))
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _f32(a, size=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if size is not None and a.size != size:
+        raise ValueError(f"expected {size} floats, got {a.size}")
+    return a
+
+
+def block_features(**info) -> np.ndarray:
+    """The 32 features of a block (the library's host-side copy of the planner's function)."""
+    b = BlockInfo()
+    for k, v in info.items():
+        setattr(b, k, int(v))
+    out = np.zeros(SCORER_FEATURES, dtype=np.float32)
+    lib().ltlg_block_features(C.byref(b), _fp(out))
+    return out
+
+
+def scorer_forward(params: np.ndarray, features: np.ndarray) -> np.ndarray:
+    """Logits of the scorer on the device (BF16 operands, FP32 sums)."""
+    p = _f32(params, SCORER_PARAMS)
+    x = _f32(features).reshape(-1, SCORER_FEATURES)
+    out = np.zeros(x.shape[0], dtype=np.float32)
+    rc = lib().ltlg_scorer_forward(_fp(p), _fp(x), x.shape[0], _fp(out))
+    if rc != 0:
+        raise RuntimeError(f"scorer_forward failed: {status_string(rc)}")
+    return out
+
+
+def scorer_grad(params: np.ndarray, features: np.ndarray, labels: np.ndarray, pos_weight: float = 1.0):
+    """Gradient (and loss) of the mean weighted binary cross-entropy, computed on the device."""
+    p = _f32(params, SCORER_PARAMS)
+    x = _f32(features).reshape(-1, SCORER_FEATURES)
+    y = _f32(labels)
+    g = np.zeros(SCORER_PARAMS, dtype=np.float32)
+    loss = C.c_float(0.0)
+    rc = lib().ltlg_scorer_grad(_fp(p), _fp(x), _fp(y), x.shape[0], float(pos_weight), _fp(g), C.byref(loss))
+    if rc != 0:
+        raise RuntimeError(f"scorer_grad failed: {status_string(rc)}")
+    return g, loss.value
+
+
+def scorer_train(params: np.ndarray, features: np.ndarray, labels: np.ndarray, epochs=30, batch=1024, lr=2e-3,
+                 pos_weight=1.0, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=0.0, seed=0):
+    """Adam training on the device; returns (new params, per-epoch mean loss)."""
+    p = _f32(params, SCORER_PARAMS).copy()
+    x = _f32(features).reshape(-1, SCORER_FEATURES)
+    y = _f32(labels)
+    cfg = TrainConfig(int(epochs), int(batch), float(lr), float(pos_weight), float(beta1), float(beta2), float(eps),
+                      float(weight_decay), int(seed))
+    curve = np.zeros(max(int(epochs), 1), dtype=np.float32)
+    rc = lib().ltlg_scorer_train(_fp(p), _fp(x), _fp(y), x.shape[0], C.byref(cfg), _fp(curve))
+    if rc != 0:
+        raise RuntimeError(f"scorer_train failed: {status_string(rc)}")
+    return p, curve[:int(epochs)]
 
 
 def device_apply_op(op: int, a: np.ndarray, b: np.ndarray | None, lenmask: np.ndarray):

@@ -74,6 +74,8 @@ struct ltlg_engine {
     // arguments from `args`, so the graphs stay valid from one learn to the next; they are
     // captured again only when the kernel instances or grids change (graph_key).
     cudaGraphExec_t level_graph[RING] = {};
+    DevBuf scorer, scorer_params;   // the learned block order's scorer (MlpDev, packed FP32)
+    bool has_scorer = false;
     long long graph_key[8] = {};
     DevBuf h_ctl, h_walk, h_stage, h_snaps, h_args, h_lev, h_ls, h_lcands, h_win, h_ring;
 
@@ -129,6 +131,21 @@ std::vector<Block> level_blocks(int c, const int *cf, int neg_type, const std::v
     if (c - cf[6] >= c1) unary(OP_G, c - cf[6]);
     binary(OP_U, cf[7]);
     return out;
+}
+
+// The window of block (op, k) in a host copy of a plan: items [lo, hi) of the level's item
+// table (unary blocks must be unfused, one per operator).
+void block_window(const DevLevel *hl, int op, int k, long long &lo, long long &hi) {
+    const bool un = op == OP_NEG || op == OP_X || op == OP_F || op == OP_G;
+    for (int r = 0; r < hl->nranges; ++r) {
+        const ItemRange &R = hl->ranges[r];
+        if (un ? (R.cls == 1 && hl->ublocks[R.idx].op == op) : (R.cls != 1 && R.idx == op * MAX_SPLITS + k)) {
+            lo = R.item0;
+            hi = r + 1 < hl->nranges ? hl->ranges[r + 1].item0 : hl->items_end;
+            return;
+        }
+    }
+    lo = hi = 0;
 }
 
 int cost_of_row(const std::vector<long long> &ls, long long row) {
@@ -284,7 +301,7 @@ LTLG_API void ltlg_engine_destroy(ltlg_engine *e) {
     for (cudaGraphExec_t g : e->level_graph)
         if (g) cudaGraphExecDestroy(g);
     for (DevBuf *b : {&e->cache, &e->parents, &e->keys, &e->slots, &e->wmeta, &e->kmeta, &e->ctl, &e->walk, &e->snaps,
-                      &e->lev, &e->ls, &e->lcands, &e->args})
+                      &e->lev, &e->ls, &e->lcands, &e->args, &e->scorer, &e->scorer_params})
         if (b->p) cudaFree(b->p);
     for (DevBuf *b : {&e->h_ctl, &e->h_walk, &e->h_stage, &e->h_snaps, &e->h_args, &e->h_lev, &e->h_ls, &e->h_lcands,
                       &e->h_win, &e->h_ring})
@@ -327,7 +344,9 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     const int nalpha = (int)alpha.size();
     const bool ref_keys = opt->key_mode == LTLG_KEY_REF;
     if (npos < 0 || nneg < 0 || (ref_keys && (opt->rlx_unq_chk_type < 1 || opt->rlx_unq_chk_type > 3)) ||
-        opt->key_mode < 0 || opt->key_mode > 2 || n > e->cfg.max_traces || nalpha > 26) {
+        opt->key_mode < 0 || opt->key_mode > 2 || n > e->cfg.max_traces || nalpha > 26 ||
+        (opt->order != LTLG_ORDER_PLAIN && opt->order != LTLG_ORDER_LEARNED) ||
+        (opt->order == LTLG_ORDER_LEARNED && !e->has_scorer)) {
         res->status = LTLG_BAD_ARGS;
         res->formula = strdup("bad_arguments");
         return res->status;
@@ -508,11 +527,14 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     A.lev = dlev;
     A.ls = (long long *)e->ls.p;
     A.level_cands = (u64 *)e->lcands.p;
+    A.model = opt->order == LTLG_ORDER_LEARNED ? e->scorer.p : nullptr;
     cudaMemsetAsync(e->ls.p, 0, (MAX_COSTS + 2) * sizeof(long long), st);
     cudaMemsetAsync(e->lcands.p, 0, (MAX_COSTS + 2) * sizeof(u64), st);
     DevLevel *hl = (DevLevel *)e->h_lev.p;
     memset(hl, 0, offsetof(DevLevel, blocks));
     hl->cost = c1;  // the planner advances to c1 + 1 first
+    hl->plan_flags = (opt->schedule == LTLG_SCHEDULE_PER_BLOCK ? PLAN_UNFUSED : 0) |
+                     (opt->order == LTLG_ORDER_LEARNED ? PLAN_LEARNED : 0);
     cudaMemcpyAsync(dlev, hl, offsetof(DevLevel, blocks), cudaMemcpyHostToDevice, st);
     const LevelArgs *dA = (const LevelArgs *)e->args.p;
     cudaMemcpyAsync(e->args.p, ha, sizeof(LevelArgs), cudaMemcpyHostToDevice, st);
@@ -664,30 +686,20 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
             DevCtl *dctl = (DevCtl *)e->ctl.p;
             if (per_block) {
                 // one launch per block in the reference's order, each after a snapshot; the
-                // block's items are its window of the level kernel's item space (a unary block
-                // is copied into ublocks[0], items [0, its items))
-                long long base[7];
-                base[OP_NEG] = base[OP_X] = base[OP_F] = base[OP_G] = 0;
-                base[OP_AND] = hl->win_hi[1];
-                base[OP_OR] = hl->win_hi[1] + hl->total_items[OP_AND];
-                base[OP_U] = hl->win_hi[1] + hl->win_hi[2];
+                // block's items are its window of the level's item table (unfused unary blocks)
                 size_t nb_level = 0;
                 for (int op = 0; op < 7; ++op) {
-                    const bool un = op == OP_NEG || op == OP_X || op == OP_F || op == OP_G;
                     for (int k = 0; k < hl->nblocks[op]; ++k) {
-                        const BlockDesc &B = hl->blocks[op][k];
                         cudaMemcpyAsync((DevCtl *)e->snaps.p + nb_level, e->ctl.p, sizeof(DevCtl),
                                         cudaMemcpyDeviceToDevice, st);
                         long long *win = (long long *)e->h_win.p + 8 * nb_level;
-                        const long long lo = un ? 0 : base[op] + B.item0, hi = lo + B.items;
+                        long long lo = 0, hi = 0;
+                        block_window(hl, op, k, lo, hi);
                         win[0] = lo;  // queue[0]
-                        win[1] = hi;  // win_hi[0]
-                        if (un)  // the level kernel's unary items come from ublocks: this block alone
-                            cudaMemcpyAsync(&dlev->ublocks[0], &dlev->blocks[op][k], sizeof(BlockDesc),
-                                            cudaMemcpyDeviceToDevice, st);
+                        win[1] = hi;  // items_end
                         cudaMemcpyAsync(&dctl->queue[0], &win[0], sizeof(u64), cudaMemcpyHostToDevice, st);
-                        cudaMemcpyAsync(&dlev->win_hi[0], &win[1], sizeof(long long), cudaMemcpyHostToDevice, st);
-                        const int grid = (int)std::min<long long>(B.items, max_grid);
+                        cudaMemcpyAsync(&dlev->items_end, &win[1], sizeof(long long), cudaMemcpyHostToDevice, st);
+                        const int grid = (int)std::max<long long>(1, std::min<long long>(hi - lo, max_grid));
                         if ((err = launch_level(A, dA, grid, block_threads, st)) != cudaSuccess)
                             return fail_cuda(e, err, res);
                         ++launches;
@@ -695,8 +707,8 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
                     }
                 }
             } else {
-                if (hl->win_hi[0] > 0) {
-                    const int grid = (int)std::min<long long>(hl->win_hi[0], max_grid);
+                if (hl->items_end > 0) {
+                    const int grid = (int)std::min<long long>(hl->items_end, max_grid);
                     if ((err = launch_level(A, dA, grid, block_threads, st)) != cudaSuccess)
                         return fail_cuda(e, err, res);
                     ++launches;
@@ -867,6 +879,130 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
 
 LTLG_API void *ltlg_engine_stream(ltlg_engine *e) { return e ? (void *)e->stream : nullptr; }
 
+LTLG_API void ltlg_block_features(const ltlg_block_info *in, float *f) {
+    BlockInfo b{};
+    b.op = in->op;
+    b.cost = in->cost;
+    b.c1 = in->c1;
+    b.lcost = in->lcost;
+    b.rcost = in->rcost;
+    b.position = in->position;
+    b.nblocks = in->nblocks;
+    b.lrows = in->lrows;
+    b.rrows = in->rrows;
+    b.candidates = in->candidates;
+    b.level_cands = in->level_cands;
+    b.u_left = in->u_left;
+    b.u_right = in->u_right;
+    b.c_left = in->c_left;
+    b.c_right = in->c_right;
+    b.u_prev = in->u_prev;
+    b.c_prev = in->c_prev;
+    b.npos = in->npos;
+    b.nneg = in->nneg;
+    b.nalpha = in->nalpha;
+    block_features(b, f);
+}
+
+LTLG_API int ltlg_engine_set_scorer(ltlg_engine *e, const float *params, int32_t count) {
+    if (!e || !params || count != MLP_PARAMS) return LTLG_BAD_ARGS;
+    cudaSetDevice(e->cfg.device);
+    cudaError_t err = ensure(e->scorer_params, MLP_PARAMS * sizeof(float));
+    if (err == cudaSuccess) err = ensure(e->scorer, sizeof(MlpDev));
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(e->scorer_params.p, params, MLP_PARAMS * sizeof(float), cudaMemcpyHostToDevice, e->stream);
+    if (err == cudaSuccess) err = launch_scorer_pack((const float *)e->scorer_params.p, (MlpDev *)e->scorer.p, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) return fail_cuda(e, err, nullptr);
+    e->has_scorer = true;
+    return 0;
+}
+
+LTLG_API int ltlg_engine_label_blocks(ltlg_engine *e, const ltlg_traces *t, const ltlg_options *opt_in,
+                                      ltlg_block_record *rec, int32_t cap, int32_t *count, ltlg_result *res) {
+    if (!e || !t || !opt_in || !count || !res || cap < 0 || (cap > 0 && !rec)) return LTLG_BAD_ARGS;
+    *count = 0;
+    ltlg_options opt = *opt_in;
+    opt.stop_at_found = 1;
+    opt.order = LTLG_ORDER_PLAIN;
+    opt.schedule = LTLG_SCHEDULE_FUSED;
+    const int rc = ltlg_engine_learn(e, t, &opt, res);
+    if (rc != LTLG_FOUND || res->found_op == OP_ATOM || res->on_the_fly) return rc;
+    const int c = res->cost;
+    const int *cf = opt.cost_fun;
+    cudaStream_t st = e->stream;
+    const LevelArgs &A = *(const LevelArgs *)e->h_args.p;
+    const LevelArgs *dA = (const LevelArgs *)e->args.p;
+    const std::vector<long long> &ls = e->level_start;
+    if ((int)ls.size() < c + 2) return rc;
+    // Back to the start of level c: the rows of the lower levels (the level starts below c
+    // are still on the device), a clean control block, and a check-only plan of level c with
+    // one block per operator.
+    DevCtl *hc = (DevCtl *)e->h_ctl.p;
+    memset(hc, 0, sizeof(DevCtl));
+    hc->row_count = (u64)ls[c];
+    DevLevel *hl = (DevLevel *)e->h_lev.p;
+    memset(hl, 0, offsetof(DevLevel, blocks));
+    hl->cost = c - 1;
+    hl->on_the_fly = 1;
+    hl->plan_flags = PLAN_UNFUSED;
+    DevLevel *dlev = (DevLevel *)e->lev.p;
+    DevCtl *dctl = (DevCtl *)e->ctl.p;
+    cudaMemcpyAsync(dctl, hc, sizeof(DevCtl), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dlev, hl, offsetof(DevLevel, blocks), cudaMemcpyHostToDevice, st);
+    cudaError_t err = launch_plan(dA, st);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(hl, dlev, sizeof(DevLevel), cudaMemcpyDeviceToHost, st);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(e->h_lcands.p, e->lcands.p, (MAX_COSTS + 2) * sizeof(u64), cudaMemcpyDeviceToHost, st);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    if (err != cudaSuccess) return fail_cuda(e, err, nullptr);
+    if (hl->halt) return rc;
+    const long long max_grid = (long long)e->num_sms *
+                               std::max(1, level_kernel_max_ctas_per_sm(A.left_tile, A.hash_kind, e->cfg.block_threads, A.pitch));
+    // One launch per block: clear the find, open the block's window, run, read the find.
+    long long *win = (long long *)e->h_win.p;
+    int nb = 0;
+    for (int op = 0; op < 7; ++op)
+        for (int k = 0; k < hl->nblocks[op]; ++k, ++nb) {
+            long long lo = 0, hi = 0;
+            block_window(hl, op, k, lo, hi);
+            long long *w = win + 8 * nb;
+            w[0] = lo;
+            w[1] = hi;
+            w[2] = 0;
+            cudaMemsetAsync(&dctl->found, 0, sizeof(u64), st);
+            cudaMemcpyAsync(&dctl->queue[0], &w[0], sizeof(u64), cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(&dlev->items_end, &w[1], sizeof(long long), cudaMemcpyHostToDevice, st);
+            const int grid = (int)std::max<long long>(1, std::min<long long>(hi - lo, max_grid));
+            if ((err = launch_level(A, dA, grid, e->cfg.block_threads, st)) != cudaSuccess) return fail_cuda(e, err, nullptr);
+            cudaMemcpyAsync(&w[2], &dctl->found, sizeof(u64), cudaMemcpyDeviceToHost, st);
+        }
+    if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, nullptr);
+    const u64 *lc = (const u64 *)e->h_lcands.p;
+    int nbl = 0;
+    for (int q = 0; q < 7; ++q) nbl += hl->nblocks[q];
+    nb = 0;
+    int out = 0;
+    for (int op = 0; op < 7; ++op)
+        for (int k = 0; k < hl->nblocks[op]; ++k, ++nb) {
+            if (out >= cap) continue;
+            const BlockDesc &b = hl->blocks[op][k];
+            const BlockInfo bi =
+                block_info(b, op, c, cf, nbl, (long long)hl->level_cands, ls.data(), lc, A.npos, A.n, A.nalpha);
+            ltlg_block_record &r = rec[out++];
+            r.cost = c;
+            r.op = op;
+            r.lcost = bi.lcost;
+            r.rcost = bi.rcost;
+            r.position = b.pad;
+            r.won = win[8 * nb + 2] != 0 ? 1 : 0;
+            r.candidates = b.candidates;
+            block_features(bi, r.features);
+        }
+    *count = out;
+    return rc;
+}
+
 LTLG_API int ltlg_learn(const ltlg_traces *t, const ltlg_options *opt, ltlg_result *res) {
     ltlg_engine_config cfg;
     ltlg_default_engine_config(&cfg);
@@ -946,6 +1082,15 @@ LTLG_API int ltlg_batch_learn(ltlg_batch *b, const ltlg_traces *traces, int32_t 
     for (int i = 0; i < count; ++i)
         if (results[i].status != LTLG_FOUND && results[i].status != LTLG_NOT_FOUND && !rc) rc = results[i].status;
     return rc;
+}
+
+LTLG_API int ltlg_batch_set_scorer(ltlg_batch *b, const float *params, int32_t count) {
+    if (!b) return LTLG_BAD_ARGS;
+    for (ltlg_engine *e : b->engines) {
+        const int rc = ltlg_engine_set_scorer(e, params, count);
+        if (rc != 0) return rc;
+    }
+    return 0;
 }
 
 LTLG_API int ltlg_engine_read_rows(ltlg_engine *e, int64_t first, int64_t count, uint64_t *rows, uint64_t *parents) {

@@ -662,6 +662,20 @@ __device__ __noinline__ void unary_item(const LevelArgs &A, const BlockDesc &B, 
     }
 }
 
+// Copy the arguments and the level's plan header into shared memory (thread 0).
+__device__ __forceinline__ void load_level(LevelArgs &A, const LevelArgs *A0) {
+    A = *A0;
+    const DevLevel *L = A.lev;
+    A.cost = L->cost;
+    A.check_only = L->check_only;
+    A.right_chunk = L->right_chunk;
+    A.unary_rows = L->unary_rows;
+}
+
+// Leading entries of the item table kept in shared memory (read once per item in a learned
+// order).  Small enough that three CTAs with a 64 KB tile still fit the 196 KB carveout.
+constexpr int RANGE_CACHE = 32;
+
 __device__ __forceinline__ int find_block(const BlockDesc *blocks, int nb, long long in_op) {
     int lo = 0, hi = nb - 1;
     while (lo < hi) {
@@ -674,29 +688,22 @@ __device__ __forceinline__ int find_block(const BlockDesc *blocks, int nb, long 
     return lo;
 }
 
-// Copy the arguments and the level's plan header into shared memory (thread 0).
-__device__ __forceinline__ void load_level(LevelArgs &A, const LevelArgs *A0) {
-    A = *A0;
-    const DevLevel *L = A.lev;
-    A.cost = L->cost;
-    A.check_only = L->check_only;
-    A.right_chunk = L->right_chunk;
-    A.unary_rows = L->unary_rows;
-}
-
 // One level: every work item of the plan in A.lev, drained through one queue
-// (ctl->queue[0] up to lev->win_hi[0]).  Item space: the fused unary blocks (win_hi[1]
-// items), then the & and | blocks (win_hi[2]), then the U blocks (win_hi[3]).  A binary item
-// stages a tile of left rows in shared memory with one bulk copy; the CTA's warps take the
-// item's right rows one at a time.
+// (ctl->queue[0] up to lev->items_end).  Items are numbered in the plain order: the unary
+// blocks' items, then the & blocks', the | blocks', the U blocks'.  Under a learned order the
+// queue runs through the item table instead and thread 0 maps each claimed item to its plain
+// number.  A unary item is A.unary_rows source rows of a unary block (every operator of its
+// mask on each row); a binary item stages a tile of left rows in shared memory with one bulk
+// copy, and the CTA's warps take the item's right rows one at a time.
 template <int TL, int HK>
 __global__ void __launch_bounds__(256, 3) level_kernel(const LevelArgs *__restrict__ A0) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     u64 *tile = reinterpret_cast<u64 *>(smem_raw);
     __shared__ __align__(16) LevelArgs A;
     __shared__ __align__(8) u64 bar;
+    __shared__ ItemRange s_rng[RANGE_CACHE];
     __shared__ long long s_item, s_hi, s_ub[5], s_cls[4], s_and;
-    __shared__ int s_halt, s_nub, s_nb[7];
+    __shared__ int s_halt, s_nub, s_nb[7], s_nr, s_learned;
     __shared__ unsigned s_next_row;
     __shared__ u64 s_evals;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -704,7 +711,7 @@ __global__ void __launch_bounds__(256, 3) level_kernel(const LevelArgs *__restri
         load_level(A, A0);
         const DevLevel *L = A.lev;
         s_halt = L->halt;
-        s_hi = L->win_hi[0];
+        s_hi = L->items_end;
         s_nub = L->nublocks;
         long long b = 0;
         for (int k = 0; k < 4; ++k) {
@@ -713,25 +720,39 @@ __global__ void __launch_bounds__(256, 3) level_kernel(const LevelArgs *__restri
         }
         s_ub[4] = b;
         s_cls[0] = 0;
-        s_cls[1] = L->win_hi[1];
-        s_cls[2] = s_cls[1] + L->win_hi[2];
-        s_cls[3] = s_cls[2] + L->win_hi[3];
+        s_cls[1] = b;
+        s_cls[2] = s_cls[1] + L->total_items[OP_AND] + L->total_items[OP_OR];
+        s_cls[3] = s_cls[2] + L->total_items[OP_U];
         s_and = L->total_items[OP_AND];
         for (int op = 0; op < 7; ++op) s_nb[op] = L->nblocks[op];
+        s_nr = L->nranges;
+        s_learned = L->learned_order;
         mbar_init(&bar, 1);
         fence_mbar_init();
         s_evals = 0;
     }
     __syncthreads();
     if (s_halt || s_hi <= 0) return;
+    if (s_learned) {
+        for (int e = threadIdx.x; e < s_nr && e < RANGE_CACHE; e += blockDim.x) s_rng[e] = A.lev->ranges[e];
+        __syncthreads();
+    }
     u64 evals = 0;
     u32 phase = 0;
+    int cur = 0;  // thread 0, learned order: table entry of the last item (claimed in increasing order)
     for (;;) {
         if (threadIdx.x == 0) {
             long long it = -1;
             if (!found_stop(A)) {
                 it = (long long)atomicAdd(&A.ctl->queue[0], 1ull);
                 if (it >= s_hi) it = -1;
+            }
+            if (it >= 0 && s_learned) {  // the entry holding the item: the last one with item0 <= it
+                const ItemRange *rng = A.lev->ranges;
+                auto item0_of = [&](int e) { return e < RANGE_CACHE ? s_rng[e].item0 : rng[e].item0; };
+                while (cur + 1 < s_nr && item0_of(cur + 1) <= it) ++cur;
+                const ItemRange R = cur < RANGE_CACHE ? s_rng[cur] : rng[cur];
+                it = R.plain0 + (it - R.item0);
             }
             s_item = it;
             s_next_row = 0;
@@ -763,144 +784,6 @@ __global__ void __launch_bounds__(256, 3) level_kernel(const LevelArgs *__restri
     if (lane == 0 && evals) atomicAdd(&s_evals, evals);
     __syncthreads();
     if (threadIdx.x == 0 && s_evals) atomicAdd(&A.ctl->evaluated, s_evals);
-}
-
-// The planner: one thread turns the level starts into the next level's plan, in the
-// reference's order (ltli6463.cu:1209-1440; NegType rule :1212): ~, & splits, | splits,
-// X, F, G, U splits; a split i pairs cost i with cost c - i - c_op, i = c1 .. (c - c_op)/2.
-__global__ void plan_kernel(const LevelArgs *__restrict__ pA) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const LevelArgs &A = *pA;
-    DevLevel *L = A.lev;
-    DevCtl *C = A.ctl;
-    if (L->halt == 2) return;  // an over-long plan stops the rest of the graph
-    const int c = L->cost + 1;
-    L->cost = c;
-    const long long rows = min((long long)C->row_count, A.cap_rows);
-    if (c < MAX_COSTS + 1) A.ls[c] = rows;  // level c - 1 ended here
-    u32 bad = ST_WAIT | ST_TABLE | ST_TMA;
-    if (!L->on_the_fly) bad |= ST_OVERFLOW;
-    const bool halt = c > A.max_cost || c >= MAX_COSTS || (A.stop_at_found && C->found != 0ull) ||
-                      (C->status & bad) != 0u;
-    for (int k = 0; k < 8; ++k) {
-        L->nblocks[k] = 0;
-        L->total_items[k] = 0;
-        L->item_hi[k] = 0;
-        C->queue[k] = 0;
-    }
-    L->item_hi_all = 0;
-    L->nublocks = 0;
-    for (int k = 0; k < 4; ++k) L->win_hi[k] = 0;
-    L->halt = halt ? 1 : 0;
-    L->level_cands = 0;
-    if (halt) return;
-    const int c1 = A.cf[0];
-    auto lo = [&](int k) { return (k >= 0 && k < c) ? A.ls[k] : 0ll; };
-    auto hi = [&](int k) { return (k >= 0 && k < c) ? A.ls[k + 1] : 0ll; };
-    u64 cands = 0;
-    bool overfull = false;
-    auto add = [&](int op, int lc, long long l0, long long l1, long long r0, long long r1, long long n) {
-        const int k = L->nblocks[op];
-        if (k >= MAX_SPLITS) {
-            overfull = true;
-            return;
-        }
-        BlockDesc &b = L->blocks[op][k];
-        b.op = op;
-        b.lcost = lc;
-        b.opmask = op == OP_NEG ? 1 : op == OP_X ? 2 : op == OP_F ? 4 : op == OP_G ? 8 : 0;
-        b.pad = 0;
-        b.l0 = l0;
-        b.l1 = l1;
-        b.r0 = r0;
-        b.r1 = r1;
-        b.candidates = n;
-        L->nblocks[op] = k + 1;
-        cands += (u64)n;
-    };
-    auto unary = [&](int op, int k) {
-        const long long a = lo(k), b = hi(k);
-        if (b > a) add(op, k, 0, 0, a, b, b - a);
-    };
-    auto binary = [&](int op, int cop) {
-        for (int i = c1; 2 * i <= c - cop; ++i) {
-            const int j = c - i - cop;
-            const long long a = lo(i), b = hi(i), x = lo(j), y = hi(j);
-            if (b > a && y > x) add(op, i, a, b, x, y, (op == OP_U ? 2 : 1) * (b - a) * (y - x));
-        }
-    };
-    const int *cf = A.cf;
-    if ((A.neg_type == 1 && c - cf[1] >= c1) || (A.neg_type == 2 && c - cf[1] == c1)) unary(OP_NEG, c - cf[1]);
-    binary(OP_AND, cf[2]);
-    binary(OP_OR, cf[3]);
-    if (c - cf[4] >= c1) unary(OP_X, c - cf[4]);
-    if (c - cf[5] >= c1) unary(OP_F, c - cf[5]);
-    if (c - cf[6] >= c1) unary(OP_G, c - cf[6]);
-    binary(OP_U, cf[7]);
-    if (overfull) {  // more splits than a plan holds: hand the level back to the host
-        for (int k = 0; k < 8; ++k) L->nblocks[k] = 0;
-        L->halt = 2;
-        return;
-    }
-    // Work-item size: a small level is cut into one right row (or one group of source rows)
-    // per warp so every SM takes part; a large level keeps the configured sizes.
-    const bool small = (long long)cands < A.small_level;
-    const int rc = small ? A.nwarps : A.right_chunk_big;
-    const int ur = small ? A.nwarps * UNARY_ROWS : A.unary_rows_big;
-    L->right_chunk = rc;
-    L->unary_rows = ur;
-    L->check_only = L->on_the_fly;
-    L->level_cands = cands;
-    if (c < MAX_COSTS + 1) A.level_cands[c] = cands;
-    // Unary operators over the same source rows become one fused block.
-    L->nublocks = 0;
-    for (int j = 0; j < 4; ++j) {
-        const int op = unary_slot_op(j);
-        if (L->nblocks[op] == 0) continue;
-        const BlockDesc &b = L->blocks[op][0];
-        int u = 0;
-        while (u < L->nublocks && !(L->ublocks[u].r0 == b.r0 && L->ublocks[u].r1 == b.r1)) ++u;
-        if (u == L->nublocks) {
-            BlockDesc &f = L->ublocks[L->nublocks++];
-            f = b;
-            f.opmask = 0;
-            f.candidates = 0;
-        }
-        L->ublocks[u].opmask |= 1 << j;
-        L->ublocks[u].candidates += b.candidates;
-    }
-    for (int u = 0; u < L->nublocks; ++u) {
-        BlockDesc &f = L->ublocks[u];
-        f.item0 = L->win_hi[1];
-        f.items = (f.r1 - f.r0 + ur - 1) / ur;
-        f.tiles_r = 1;
-        L->win_hi[1] += f.items;
-        L->item_hi_all += f.items;
-    }
-    for (int op = 0; op < 7; ++op) {
-        long long items = 0;
-        const bool bin = op == OP_AND || op == OP_OR || op == OP_U;
-        const int tile = op == OP_U ? A.left_tile / 2 : A.left_tile;
-        for (int k = 0; k < L->nblocks[op]; ++k) {
-            BlockDesc &b = L->blocks[op][k];
-            b.item0 = items;
-            if (bin) {
-                b.tiles_r = (b.r1 - b.r0 + rc - 1) / rc;
-                b.items = ((b.l1 - b.l0 + tile - 1) / tile) * b.tiles_r;
-            } else {
-                b.tiles_r = 1;
-                b.items = (b.r1 - b.r0 + ur - 1) / ur;  // items of this operator alone (per-block runs)
-            }
-            items += b.items;
-        }
-        L->total_items[op] = items;
-        L->item_hi[op] = items;
-        if (bin) {
-            L->item_hi_all += items;
-            L->win_hi[op == OP_U ? 3 : 2] += items;
-        }
-    }
-    L->win_hi[0] = L->item_hi_all;
 }
 
 // Letters: register rows [0, nalpha) in the hash set (duplicate letters stay rows,
@@ -1098,11 +981,6 @@ cudaError_t launch_level(const LevelArgs &a, const LevelArgs *d, int grid, int b
 int level_kernel_max_ctas_per_sm(int left_tile, int hash_kind, int block, int pitch) {
     if (hash_kind == 1) return left_tile == 4 ? occupancy_tl<4, 1>(block, pitch) : occupancy_tl<8, 1>(block, pitch);
     return left_tile == 4 ? occupancy_tl<4, 0>(block, pitch) : occupancy_tl<8, 0>(block, pitch);
-}
-
-cudaError_t launch_plan(const LevelArgs *d, cudaStream_t s) {
-    plan_kernel<<<1, 32, 0, s>>>(d);
-    return cudaGetLastError();
 }
 
 cudaError_t launch_insert_letters(const LevelArgs &a, const LevelArgs *d, int nalpha, cudaStream_t s) {

@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "order.cuh"
+
 namespace ltlg {
 
 using u64 = unsigned long long;
@@ -46,7 +48,7 @@ struct BlockDesc {
     int op;
     int lcost;           // cost of the left operand (unary: of the operand)
     int opmask;          // fused unary blocks: bit 0 ~, 1 X, 2 F, 3 G over the same source rows
-    int pad;
+    int pad;             // position of the block in the reference's order within its level
     long long l0, l1, r0, r1;
     long long item0;     // first work item of this block within its operator
     long long items;     // work items of this block
@@ -55,8 +57,22 @@ struct BlockDesc {
 };
 
 constexpr int MAX_SPLITS = 64;   // blocks per operator and level in a device-planned level
+constexpr int MAX_RANGES = 4 + 3 * MAX_SPLITS;  // entries of a level's item table
 constexpr int UNARY_ROWS = 2;    // source rows per unary work item (each with every operator of its mask)
 constexpr int MAX_COSTS = 512;   // level starts kept on the device
+
+// One entry of a level's item table: a block and where its items start.
+struct ItemRange {
+    long long item0;     // first item of the entry in the order the queue runs
+    long long plain0;    // the same item's number in the plain order
+    int cls;             // 1 unary (ublocks[idx]), 2 & or | (blocks[idx / MAX_SPLITS][idx % MAX_SPLITS]), 3 U
+    int idx;
+};
+
+enum : int {
+    PLAN_UNFUSED = 1,    // one unary block per operator (per-block runs, learned order, labels)
+    PLAN_LEARNED = 2,    // order the item table by the scorer (LevelArgs::model), highest first
+};
 
 // The plan of the level being enumerated, in device memory.  The planner kernel writes it
 // from the level starts; the host writes it directly in the per-block schedule.
@@ -66,18 +82,24 @@ struct DevLevel {
     int check_only;      // on-the-fly: acceptance only, no dedupe, no storing
     int on_the_fly;      // set by the host: plan check-only levels and ignore the overflow bit
     long long item_hi_all;  // all work items of the level
-    long long win_hi[4];    // [0]: the level kernel takes items from ctl->queue[0] below it; [1..3]: items of
-                            // the fused unary blocks, of the & and | blocks, of the U blocks
+    long long items_end;    // the level kernel takes items from ctl->queue[0] below it
     int right_chunk;
     int unary_rows;
     int nblocks[8];
     long long total_items[8];
     long long item_hi[8];  // an operator kernel takes items from its queue until item_hi
     u64 level_cands;     // candidates of the level, counted as the reference counts them
-    int nublocks;        // fused unary blocks: the unary kernel works from these
-    int pad2;
+    int plan_flags;      // set by the host: PLAN_* bits
+    int nublocks;        // unary blocks the level kernel works from (fused over operators
+                         // unless PLAN_UNFUSED)
     BlockDesc ublocks[4];
     BlockDesc blocks[7][MAX_SPLITS];
+    // The level's blocks in the order the queue runs: entry e covers queue items
+    // [ranges[e].item0, ranges[e + 1].item0) (the last one up to items_end).
+    int nranges;
+    int learned_order;   // 1: the table is sorted by score and the queue runs through it
+    ItemRange ranges[MAX_RANGES];
+    float scores[MAX_RANGES];  // PLAN_LEARNED: the scorer's logit of each entry
 };
 
 struct LevelArgs {
@@ -110,12 +132,47 @@ struct LevelArgs {
     DevLevel *lev;
     long long *ls;       // level starts: rows of cost c are [ls[c], ls[c + 1])
     u64 *level_cands;    // per cost
+    const void *model;   // PLAN_LEARNED: the scorer (MlpDev)
     // per level (filled into the shared copy from the plan)
     int cost;
     int check_only;
     int right_chunk;
     int unary_rows;
 };
+
+// The feature inputs of block b (operator op) of level c: the same code on the device
+// (planner) and on the host (training records).  ls[k] is the first row of cost k, lcands[k]
+// the candidates of level k (0 for the letter level).
+__host__ __device__ inline BlockInfo block_info(const BlockDesc &b, int op, int c, const int *cf, int nblocks,
+                                                long long level_cands, const long long *ls, const u64 *lcands,
+                                                int npos, int n, int nalpha) {
+    const bool un = op == OP_NEG || op == OP_X || op == OP_F || op == OP_G;
+    const int c1 = cf[0];
+    auto urows = [&](int k) { return (k >= 0 && k < c) ? ls[k + 1] - ls[k] : 0ll; };
+    auto ucands = [&](int k) { return (k > c1 && k < c && k < MAX_COSTS + 1) ? (long long)lcands[k] : 0ll; };
+    BlockInfo bi{};
+    bi.op = op;
+    bi.cost = c;
+    bi.c1 = c1;
+    bi.lcost = b.lcost;
+    bi.rcost = un ? 0 : c - b.lcost - cf[op + 1];
+    bi.position = b.pad;
+    bi.nblocks = nblocks;
+    bi.lrows = un ? b.r1 - b.r0 : b.l1 - b.l0;
+    bi.rrows = un ? 1 : b.r1 - b.r0;
+    bi.candidates = b.candidates;
+    bi.level_cands = level_cands;
+    bi.u_left = urows(bi.lcost);
+    bi.u_right = un ? 0 : urows(bi.rcost);
+    bi.c_left = ucands(bi.lcost);
+    bi.c_right = un ? 0 : ucands(bi.rcost);
+    bi.u_prev = urows(c - 1);
+    bi.c_prev = ucands(c - 1);
+    bi.npos = npos;
+    bi.nneg = n - npos;
+    bi.nalpha = nalpha;
+    return bi;
+}
 
 // Launch wrappers (ltl_kernels.cu).  A level is one kernel (launch_level) that drains
 // ctl->queue[0]; the planner (launch_plan) writes its plan first.  The kernels read their
@@ -127,6 +184,7 @@ cudaError_t launch_level(const LevelArgs &a, const LevelArgs *d, int grid, int b
 cudaError_t launch_plan(const LevelArgs *d, cudaStream_t s);
 cudaError_t launch_insert_letters(const LevelArgs &a, const LevelArgs *d, int nalpha, cudaStream_t s);
 cudaError_t launch_walk(const u64 *parents, int nalpha, u64 found, u64 *out, int cap, cudaStream_t s);
+cudaError_t launch_scorer_pack(const float *params, MlpDev *out, cudaStream_t s);
 cudaError_t launch_apply_op(int op, const u64 *a, const u64 *b, const u64 *wmeta, int n, int pitch, int count,
                             u64 *out, u64 *out2, u64 *fp, cudaStream_t s);
 

@@ -1,0 +1,294 @@
+// The level planner and the learned block order's scorer on the device.  Kept apart from
+// the level kernel's translation unit so the level kernel's hot code stays compact in the
+// instruction cache.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "ltl_kernels.cuh"
+
+namespace ltlg {
+namespace {
+
+constexpr unsigned FULL = 0xFFFFFFFFu;
+
+// Operator of slot j of a fused unary block: 0 ~, 1 X, 2 F, 3 G.
+__device__ __forceinline__ int unary_slot_op(int j) { return j == 0 ? OP_NEG : j == 1 ? OP_X : j == 2 ? OP_F : OP_G; }
+
+// ---------------------------------------------------------------- learned order
+__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16(x)); }
+
+// The scorer on one feature vector, one warp: lane l computes hidden units l and l + 32 of
+// each layer.  Operands are rounded to BF16, products and sums are FP32, and every unit sums
+// its inputs in index order (the same order as forward_record in mlp.cu).
+__device__ float mlp_score_warp(const MlpDev &M, const float *x, int lane) {
+    float h1[2], h2[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+        const int j = lane + 32 * u;
+        float acc = 0.0f;
+        for (int i = 0; i < ORDER_NF; ++i) acc += __bfloat162float(M.w1[j * ORDER_NF + i]) * bf16r(x[i]);
+        h1[u] = fmaxf(acc + M.b1[j], 0.0f);
+    }
+    float acc2[2] = {0.0f, 0.0f};
+#pragma unroll
+    for (int k = 0; k < ORDER_H; ++k) {
+        const float hk = bf16r(__shfl_sync(FULL, h1[k >> 5], k & 31));
+#pragma unroll
+        for (int u = 0; u < 2; ++u) acc2[u] += __bfloat162float(M.w2[(lane + 32 * u) * ORDER_H + k]) * hk;
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) h2[u] = fmaxf(acc2[u] + M.b2[lane + 32 * u], 0.0f);
+    float z = 0.0f;
+#pragma unroll
+    for (int k = 0; k < ORDER_H; ++k) {
+        const float hk = bf16r(__shfl_sync(FULL, h2[k >> 5], k & 31));
+        z += __bfloat162float(M.w3[k]) * hk;
+    }
+    return z + M.b3;
+}
+
+// The planner: thread 0 turns the level starts into the next level's plan, in the
+// reference's order (ltli6463.cu:1209-1440; NegType rule :1212): ~, & splits, | splits,
+// X, F, G, U splits; a split i pairs cost i with cost c - i - c_op, i = c1 .. (c - c_op)/2.
+// Then the item table: plain order (unary blocks, & blocks, | blocks, U blocks), or under
+// PLAN_LEARNED every block scored by one warp and the table sorted by score (ties keep the
+// reference's order).  One CTA of 256 threads.
+__global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__ pA) {
+    const LevelArgs &A = *pA;
+    DevLevel *L = A.lev;
+    DevCtl *C = A.ctl;
+    __shared__ int s_go, s_nent, s_pos[MAX_RANGES], s_order[MAX_RANGES];
+    __shared__ ItemRange s_ent[MAX_RANGES];
+    __shared__ long long s_cnt[MAX_RANGES];
+    __shared__ float s_score[MAX_RANGES];
+    __shared__ float s_x[8][ORDER_NF];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        s_go = 0;
+        s_nent = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) do {
+        if (L->halt == 2) break;  // an over-long plan stops the rest of the graph
+        const int c = L->cost + 1;
+        L->cost = c;
+        const long long rows = min((long long)C->row_count, A.cap_rows);
+        if (c < MAX_COSTS + 1) A.ls[c] = rows;  // level c - 1 ended here
+        u32 bad = ST_WAIT | ST_TABLE | ST_TMA;
+        if (!L->on_the_fly) bad |= ST_OVERFLOW;
+        const bool halt = c > A.max_cost || c >= MAX_COSTS || (A.stop_at_found && C->found != 0ull) ||
+                          (C->status & bad) != 0u;
+        for (int k = 0; k < 8; ++k) {
+            L->nblocks[k] = 0;
+            L->total_items[k] = 0;
+            L->item_hi[k] = 0;
+            C->queue[k] = 0;
+        }
+        L->item_hi_all = 0;
+        L->nublocks = 0;
+        L->nranges = 0;
+        L->learned_order = 0;
+        L->items_end = 0;
+        L->halt = halt ? 1 : 0;
+        L->level_cands = 0;
+        if (halt) break;
+        const int c1 = A.cf[0];
+        auto lo = [&](int k) { return (k >= 0 && k < c) ? A.ls[k] : 0ll; };
+        auto hi = [&](int k) { return (k >= 0 && k < c) ? A.ls[k + 1] : 0ll; };
+        u64 cands = 0;
+        bool overfull = false;
+        int nb = 0;
+        auto add = [&](int op, int lc, long long l0, long long l1, long long r0, long long r1, long long n) {
+            const int k = L->nblocks[op];
+            if (k >= MAX_SPLITS) {
+                overfull = true;
+                return;
+            }
+            BlockDesc &b = L->blocks[op][k];
+            b.op = op;
+            b.lcost = lc;
+            b.opmask = op == OP_NEG ? 1 : op == OP_X ? 2 : op == OP_F ? 4 : op == OP_G ? 8 : 0;
+            b.pad = nb++;  // position in the reference's order
+            b.l0 = l0;
+            b.l1 = l1;
+            b.r0 = r0;
+            b.r1 = r1;
+            b.candidates = n;
+            L->nblocks[op] = k + 1;
+            cands += (u64)n;
+        };
+        auto unary = [&](int op, int k) {
+            const long long a = lo(k), b = hi(k);
+            if (b > a) add(op, k, 0, 0, a, b, b - a);
+        };
+        auto binary = [&](int op, int cop) {
+            for (int i = c1; 2 * i <= c - cop; ++i) {
+                const int j = c - i - cop;
+                const long long a = lo(i), b = hi(i), x = lo(j), y = hi(j);
+                if (b > a && y > x) add(op, i, a, b, x, y, (op == OP_U ? 2 : 1) * (b - a) * (y - x));
+            }
+        };
+        const int *cf = A.cf;
+        if ((A.neg_type == 1 && c - cf[1] >= c1) || (A.neg_type == 2 && c - cf[1] == c1)) unary(OP_NEG, c - cf[1]);
+        binary(OP_AND, cf[2]);
+        binary(OP_OR, cf[3]);
+        if (c - cf[4] >= c1) unary(OP_X, c - cf[4]);
+        if (c - cf[5] >= c1) unary(OP_F, c - cf[5]);
+        if (c - cf[6] >= c1) unary(OP_G, c - cf[6]);
+        binary(OP_U, cf[7]);
+        if (overfull) {  // more splits than a plan holds: hand the level back to the host
+            for (int k = 0; k < 8; ++k) L->nblocks[k] = 0;
+            L->halt = 2;
+            break;
+        }
+        // Work-item size: a small level is cut into one right row (or one group of source
+        // rows) per warp so every SM takes part; a large level keeps the configured sizes.
+        const bool small = (long long)cands < A.small_level;
+        const int rc = small ? A.nwarps : A.right_chunk_big;
+        const int ur = small ? A.nwarps * UNARY_ROWS : A.unary_rows_big;
+        L->right_chunk = rc;
+        L->unary_rows = ur;
+        L->check_only = L->on_the_fly;
+        L->level_cands = cands;
+        if (c < MAX_COSTS + 1) A.level_cands[c] = cands;
+        const bool fuse = !(L->plan_flags & (PLAN_UNFUSED | PLAN_LEARNED));
+        // Unary blocks: one per operator, or (fused) one per distinct source range with every
+        // operator on it.
+        int nu = 0;
+        for (int j = 0; j < 4; ++j) {
+            const int op = unary_slot_op(j);
+            if (L->nblocks[op] == 0) continue;
+            const BlockDesc &b = L->blocks[op][0];
+            int u = 0;
+            while (fuse && u < nu && !(L->ublocks[u].r0 == b.r0 && L->ublocks[u].r1 == b.r1)) ++u;
+            if (!fuse || u == nu) {
+                u = nu++;
+                BlockDesc &f = L->ublocks[u];
+                f = b;
+                f.opmask = 0;
+                f.candidates = 0;
+            }
+            L->ublocks[u].opmask |= 1 << j;
+            L->ublocks[u].candidates += b.candidates;
+        }
+        L->nublocks = nu;
+        int ne = 0;
+        for (int u = 0; u < nu; ++u) {
+            BlockDesc &f = L->ublocks[u];
+            f.items = (f.r1 - f.r0 + ur - 1) / ur;
+            f.tiles_r = 1;
+            s_ent[ne] = ItemRange{f.items, 0, 1, u};
+            s_pos[ne++] = f.pad;
+        }
+        for (int op = 0; op < 7; ++op) {
+            long long items = 0;
+            const bool bin = op == OP_AND || op == OP_OR || op == OP_U;
+            const int tile = op == OP_U ? A.left_tile / 2 : A.left_tile;
+            for (int k = 0; k < L->nblocks[op]; ++k) {
+                BlockDesc &b = L->blocks[op][k];
+                b.item0 = items;
+                if (bin) {
+                    b.tiles_r = (b.r1 - b.r0 + rc - 1) / rc;
+                    b.items = ((b.l1 - b.l0 + tile - 1) / tile) * b.tiles_r;
+                    s_ent[ne] = ItemRange{b.items, 0, op == OP_U ? 3 : 2, op * MAX_SPLITS + k};
+                    s_pos[ne++] = b.pad;
+                } else {
+                    b.tiles_r = 1;
+                    b.items = (b.r1 - b.r0 + ur - 1) / ur;
+                }
+                items += b.items;
+            }
+            L->total_items[op] = items;
+            L->item_hi[op] = items;
+        }
+        s_nent = ne;  // item0 holds each entry's item count until the table is laid out
+        s_go = (L->plan_flags & PLAN_LEARNED) && A.model ? 2 : 1;
+    } while (0);
+    __syncthreads();
+    if (s_go == 0) return;
+    const int ne = s_nent;
+    if (s_go == 2) {
+        // score every entry: one warp per entry
+        const MlpDev &M = *reinterpret_cast<const MlpDev *>(A.model);
+        const int c = L->cost;
+        const int nbl = L->nblocks[0] + L->nblocks[1] + L->nblocks[2] + L->nblocks[3] + L->nblocks[4] +
+                        L->nblocks[5] + L->nblocks[6];
+        for (int e = warp; e < ne; e += blockDim.x >> 5) {
+            if (lane == 0) {
+                const ItemRange &R = s_ent[e];
+                const BlockDesc &b = R.cls == 1 ? L->ublocks[R.idx] : L->blocks[R.idx / MAX_SPLITS][R.idx % MAX_SPLITS];
+                const int op = R.cls == 1 ? b.op : R.idx / MAX_SPLITS;
+                const BlockInfo bi = block_info(b, op, c, A.cf, nbl, (long long)L->level_cands, A.ls, A.level_cands,
+                                                A.npos, A.n, A.nalpha);
+                block_features(bi, s_x[warp]);
+            }
+            __syncwarp();
+            const float z = mlp_score_warp(M, s_x[warp], lane);
+            if (lane == 0) s_score[e] = z;
+            __syncwarp();
+        }
+        __syncthreads();
+        // rank sort: highest score first, ties in the reference's order
+        for (int t = threadIdx.x; t < ne; t += blockDim.x) {
+            const float st = s_score[t];
+            int r = 0;
+            for (int j = 0; j < ne; ++j) {
+                const float sj = s_score[j];
+                r += (sj > st || (sj == st && s_pos[j] < s_pos[t])) ? 1 : 0;
+            }
+            s_order[r] = t;
+        }
+    } else {
+        for (int t = threadIdx.x; t < ne; t += blockDim.x) s_order[t] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // entries were made in the plain order: their plain starts are the prefix sums
+        long long plain = 0;
+        for (int e = 0; e < ne; ++e) {
+            const long long cnt = s_ent[e].item0;  // the entry's item count
+            s_ent[e].item0 = plain;
+            s_cnt[e] = cnt;
+            plain += cnt;
+        }
+        long long item0 = 0;
+        for (int r = 0; r < ne; ++r) {
+            const int e = s_order[r];
+            const ItemRange R = s_ent[e];
+            L->ranges[r] = ItemRange{item0, R.item0, R.cls, R.idx};
+            L->scores[r] = s_go == 2 ? s_score[e] : 0.0f;
+            item0 += s_cnt[e];
+        }
+        L->nranges = ne;
+        L->learned_order = s_go == 2 ? 1 : 0;
+        L->items_end = item0;
+        L->item_hi_all = item0;
+    }
+}
+
+// The scorer's device form from the packed FP32 parameters: weights rounded to BF16.
+__global__ void scorer_pack_kernel(const float *__restrict__ p, MlpDev *__restrict__ m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ORDER_H * ORDER_NF) m->w1[i] = __float2bfloat16(p[MLP_W1 + i]);
+    if (i < ORDER_H * ORDER_H) m->w2[i] = __float2bfloat16(p[MLP_W2 + i]);
+    if (i < ORDER_H) {
+        m->w3[i] = __float2bfloat16(p[MLP_W3 + i]);
+        m->b1[i] = p[MLP_B1 + i];
+        m->b2[i] = p[MLP_B2 + i];
+    }
+    if (i == 0) m->b3 = p[MLP_B3];
+}
+
+}  // namespace
+
+cudaError_t launch_plan(const LevelArgs *d, cudaStream_t s) {
+    plan_kernel<<<1, 256, 0, s>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scorer_pack(const float *params, MlpDev *out, cudaStream_t s) {
+    scorer_pack_kernel<<<(MLP_PARAMS + 255) / 256, 256, 0, s>>>(params, out);
+    return cudaGetLastError();
+}
+
+}  // namespace ltlg

@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--quiet-extra", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain block order comparison")
     return ap.parse_args()
 
 
@@ -181,6 +182,36 @@ def cpu_baseline(batch, sample_s: float, threads: int = 0, costs=(1,) * 8):
             "sample": f"{solved} of {len(batch)} batch instances solved in {el:.1f} s "
                       f"(CPU port of the same enumeration, OpenMP, exact uniqueness)",
             "candidate_cs_per_s": cands / el, "seconds": el}
+
+
+def learned_order_report(ekw, repeats: int = 2):
+    """Time-to-minimal-formula with the packaged learned block order against the plain order,
+    on held-out Hamming-style instances (4 propositions, 1000 positive traces of length
+    20-48, 1000 negatives each a positive with 1-3 bits flipped; hidden formula of size 9),
+    best of `repeats` per instance and order.  The minimal cost must be the same."""
+    from ltlb200 import api, learned
+    specs = [(s, 1000, 9) for s in learned.HELD_OUT_SEEDS]
+    insts = list(learned.instances(specs, workers=8, chunk=2))
+    kw = dict(ekw, slots_log2=max(ekw.get("slots_log2", 26), 26))
+    with api.Engine(**kw) as eng:
+        rows = learned.compare(eng, insts, learned.load_scorer(), repeats=repeats)
+    s = learned.summarize(rows)
+    hard = [r for r in rows if r["cost_plain"] >= 8]
+    return {
+        "workload": "cfg5 shape: 4 props, 1000 pos (len U[20,48], Bernoulli(0.5)) + 1000 negatives = positives "
+                    "with 1-3 flipped bits, hidden formula size 9; held-out seeds "
+                    f"{learned.HELD_OUT_SEEDS[0]}-{learned.HELD_OUT_SEEDS[-1]}",
+        "instances": s["instances"], "same_cost": s["same_cost"],
+        "time_to_minimal_ms": {"plain": s["ms_plain"], "learned": s["ms_learned"]},
+        "speedup": s["speedup"],
+        "device_ms": {"plain": s["device_ms_plain"], "learned": s["device_ms_learned"]},
+        "candidates_before_find": {"plain": s["evaluated_plain"], "learned": s["evaluated_learned"]},
+        "cost_ge_8": {"instances": len(hard),
+                      "speedup_total_time": (sum(r["ms_plain"] for r in hard) / max(1e-9, sum(r["ms_learned"] for r in hard)))
+                      if hard else None},
+        "per_instance": [[r["cost_plain"], round(r["ms_plain"], 3), round(r["ms_learned"], 3)] for r in rows],
+        "scorer": "scorer_hamming.npy: MLP 32-64-64-1, BF16/FP32, trained on the GPU on 198,070 block records",
+    }
 
 
 def run_reference(a):
@@ -327,6 +358,8 @@ def run_ours(a):
             "gpu_launches": launches,
             "clocks": clocks,
         }
+        if ws == 1 and not a.no_learned:
+            line["learned_order"] = learned_order_report(ekw)
         if ws == 1 and not a.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(batch, a.cpu_sample_s)
         print(json.dumps(line), flush=True)

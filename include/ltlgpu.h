@@ -228,11 +228,13 @@ typedef struct ltlg_block_record {
 } ltlg_block_record;
 
 /* What a block's features are computed from (host side; the device planner uses the same
- * function).  Costs are level costs, rows are cache rows, "c_" counts are candidates. */
+ * function).  Costs are level costs, rows are cache rows.  lstat / rstat: stored rows of the
+ * (left / right) operand level that hold at position 0 on every positive trace, and that
+ * hold at position 0 on no negative trace. */
 typedef struct ltlg_block_info {
     int32_t op, cost, c1, lcost, rcost, position, nblocks, pad_;
     int64_t lrows, rrows, candidates, level_cands;
-    int64_t u_left, u_right, c_left, c_right, u_prev, c_prev;
+    int64_t lstat[2], rstat[2];
     int32_t npos, nneg, nalpha, pad2_;
 } ltlg_block_info;
 

@@ -78,8 +78,7 @@ class BlockInfo(C.Structure):
     _fields_ = [("op", C.c_int32), ("cost", C.c_int32), ("c1", C.c_int32), ("lcost", C.c_int32),
                 ("rcost", C.c_int32), ("position", C.c_int32), ("nblocks", C.c_int32), ("pad_", C.c_int32),
                 ("lrows", C.c_int64), ("rrows", C.c_int64), ("candidates", C.c_int64), ("level_cands", C.c_int64),
-                ("u_left", C.c_int64), ("u_right", C.c_int64), ("c_left", C.c_int64), ("c_right", C.c_int64),
-                ("u_prev", C.c_int64), ("c_prev", C.c_int64), ("npos", C.c_int32), ("nneg", C.c_int32),
+                ("lstat", C.c_int64 * 2), ("rstat", C.c_int64 * 2), ("npos", C.c_int32), ("nneg", C.c_int32),
                 ("nalpha", C.c_int32), ("pad2_", C.c_int32)]
 
 
@@ -410,7 +409,10 @@ def block_features(**info) -> np.ndarray:
     """The 32 features of a block (the library's host-side copy of the planner's function)."""
     b = BlockInfo()
     for k, v in info.items():
-        setattr(b, k, int(v))
+        if k in ("lstat", "rstat"):
+            getattr(b, k)[:] = [int(x) for x in v]
+        else:
+            setattr(b, k, int(v))
     out = np.zeros(SCORER_FEATURES, dtype=np.float32)
     lib().ltlg_block_features(C.byref(b), _fp(out))
     return out

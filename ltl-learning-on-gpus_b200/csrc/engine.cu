@@ -75,6 +75,7 @@ struct ltlg_engine {
     // captured again only when the kernel instances or grids change (graph_key).
     cudaGraphExec_t level_graph[RING] = {};
     DevBuf scorer, scorer_params;   // the learned block order's scorer (MlpDev, packed FP32)
+    DevBuf lstats, h_lstats;        // row statistics per cost (LSTATS counters)
     bool has_scorer = false;
     long long graph_key[8] = {};
     DevBuf h_ctl, h_walk, h_stage, h_snaps, h_args, h_lev, h_ls, h_lcands, h_win, h_ring;
@@ -278,6 +279,8 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
     if (err == cudaSuccess) err = ensure_host(e->h_win, max_blocks * 8 * sizeof(long long));
     if (err == cudaSuccess) err = ensure_host(e->h_args, sizeof(LevelArgs));
     if (err == cudaSuccess) err = ensure(e->args, sizeof(LevelArgs));
+    if (err == cudaSuccess) err = ensure(e->lstats, (MAX_COSTS + 2) * LSTATS * sizeof(u64));
+    if (err == cudaSuccess) err = ensure_host(e->h_lstats, (MAX_COSTS + 2) * LSTATS * sizeof(u64));
     if (err == cudaSuccess) err = ensure_host(e->h_ring, ltlg_engine::RING * (sizeof(DevCtl) + sizeof(DevLevel)));
     if (err == cudaSuccess) err = ensure(e->lev, sizeof(DevLevel));
     if (err == cudaSuccess) err = ensure_host(e->h_lev, sizeof(DevLevel));
@@ -301,10 +304,10 @@ LTLG_API void ltlg_engine_destroy(ltlg_engine *e) {
     for (cudaGraphExec_t g : e->level_graph)
         if (g) cudaGraphExecDestroy(g);
     for (DevBuf *b : {&e->cache, &e->parents, &e->keys, &e->slots, &e->wmeta, &e->kmeta, &e->ctl, &e->walk, &e->snaps,
-                      &e->lev, &e->ls, &e->lcands, &e->args, &e->scorer, &e->scorer_params})
+                      &e->lev, &e->ls, &e->lcands, &e->args, &e->scorer, &e->scorer_params, &e->lstats})
         if (b->p) cudaFree(b->p);
     for (DevBuf *b : {&e->h_ctl, &e->h_walk, &e->h_stage, &e->h_snaps, &e->h_args, &e->h_lev, &e->h_ls, &e->h_lcands,
-                      &e->h_win, &e->h_ring})
+                      &e->h_win, &e->h_ring, &e->h_lstats})
         if (b->p) cudaFreeHost(b->p);
     for (cudaEvent_t ev : {e->ev_a, e->ev_b, e->ev_t0, e->ev_t1})
         if (ev) cudaEventDestroy(ev);
@@ -528,6 +531,9 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     A.ls = (long long *)e->ls.p;
     A.level_cands = (u64 *)e->lcands.p;
     A.model = opt->order == LTLG_ORDER_LEARNED ? e->scorer.p : nullptr;
+    A.grid = max_grid;
+    A.lstats = (u64 *)e->lstats.p;
+    cudaMemsetAsync(e->lstats.p, 0, (MAX_COSTS + 2) * LSTATS * sizeof(u64), st);
     cudaMemsetAsync(e->ls.p, 0, (MAX_COSTS + 2) * sizeof(long long), st);
     cudaMemsetAsync(e->lcands.p, 0, (MAX_COSTS + 2) * sizeof(u64), st);
     DevLevel *hl = (DevLevel *)e->h_lev.p;
@@ -892,12 +898,10 @@ LTLG_API void ltlg_block_features(const ltlg_block_info *in, float *f) {
     b.rrows = in->rrows;
     b.candidates = in->candidates;
     b.level_cands = in->level_cands;
-    b.u_left = in->u_left;
-    b.u_right = in->u_right;
-    b.c_left = in->c_left;
-    b.c_right = in->c_right;
-    b.u_prev = in->u_prev;
-    b.c_prev = in->c_prev;
+    for (int k = 0; k < 2; ++k) {
+        b.lstat[k] = in->lstat[k];
+        b.rstat[k] = in->rstat[k];
+    }
     b.npos = in->npos;
     b.nneg = in->nneg;
     b.nalpha = in->nalpha;
@@ -953,7 +957,8 @@ LTLG_API int ltlg_engine_label_blocks(ltlg_engine *e, const ltlg_traces *t, cons
     cudaError_t err = launch_plan(dA, st);
     if (err == cudaSuccess) err = cudaMemcpyAsync(hl, dlev, sizeof(DevLevel), cudaMemcpyDeviceToHost, st);
     if (err == cudaSuccess)
-        err = cudaMemcpyAsync(e->h_lcands.p, e->lcands.p, (MAX_COSTS + 2) * sizeof(u64), cudaMemcpyDeviceToHost, st);
+        err = cudaMemcpyAsync(e->h_lstats.p, e->lstats.p, (MAX_COSTS + 2) * LSTATS * sizeof(u64), cudaMemcpyDeviceToHost,
+                              st);
     if (err == cudaSuccess) err = cudaStreamSynchronize(st);
     if (err != cudaSuccess) return fail_cuda(e, err, nullptr);
     if (hl->halt) return rc;
@@ -978,7 +983,7 @@ LTLG_API int ltlg_engine_label_blocks(ltlg_engine *e, const ltlg_traces *t, cons
             cudaMemcpyAsync(&w[2], &dctl->found, sizeof(u64), cudaMemcpyDeviceToHost, st);
         }
     if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, nullptr);
-    const u64 *lc = (const u64 *)e->h_lcands.p;
+    const u64 *lst = (const u64 *)e->h_lstats.p;
     int nbl = 0;
     for (int q = 0; q < 7; ++q) nbl += hl->nblocks[q];
     nb = 0;
@@ -987,8 +992,7 @@ LTLG_API int ltlg_engine_label_blocks(ltlg_engine *e, const ltlg_traces *t, cons
         for (int k = 0; k < hl->nblocks[op]; ++k, ++nb) {
             if (out >= cap) continue;
             const BlockDesc &b = hl->blocks[op][k];
-            const BlockInfo bi =
-                block_info(b, op, c, cf, nbl, (long long)hl->level_cands, ls.data(), lc, A.npos, A.n, A.nalpha);
+            const BlockInfo bi = block_info(b, op, c, cf, nbl, (long long)hl->level_cands, lst, A.npos, A.n, A.nalpha);
             ltlg_block_record &r = rec[out++];
             r.cost = c;
             r.op = op;

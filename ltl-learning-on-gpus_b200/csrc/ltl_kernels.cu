@@ -103,8 +103,13 @@ __device__ __forceinline__ u64 hw(u64 w, u64 key, bool valid) {
     return valid ? fmix64(w ^ key) : 0ull;
 }
 // Bit 0 disagrees with the label (positives need 1, negatives 0); padding words are 0 with label 0.
-__device__ __forceinline__ u32 badbit(u64 w0, u64 w1, u64 m0, u64 m1) {
-    return (u32)(((w0 ^ (m0 >> 63)) | (w1 ^ (m1 >> 63))) & 1ull);
+// Acceptance at position 0, per pair of words: a positive trace where it fails (pmiss) or a
+// negative trace (padding words count as negative) where it holds (nhit).
+__device__ __forceinline__ u32 pmiss(u64 w0, u64 w1, u64 m0, u64 m1) {
+    return (u32)(((~w0 & (m0 >> 63)) | (~w1 & (m1 >> 63))) & 1ull);
+}
+__device__ __forceinline__ u32 nhit(u64 w0, u64 w1, u64 m0, u64 m1) {
+    return (u32)(((w0 & ~(m0 >> 63)) | (w1 & ~(m1 >> 63))) & 1ull);
 }
 
 __device__ __forceinline__ u64 ld_acquire(const u64 *p) {
@@ -280,13 +285,25 @@ enum { S_DONE = 0, S_PROBE = 1, S_CLAIM = 2, S_WAIT = 3, S_VERIFY = 4 };
 
 __device__ __forceinline__ bool slot_free(u64 v, u32 gen) { return v == 0 || (u32)((v >> 32) & 0xFFu) != gen; }
 
+// Per-level counts of stored rows by how they behave at position 0 (the acceptance bit):
+// [0] holds on every positive trace, [1] holds on no negative trace.  Masks: bit l set when
+// candidate l fails on some positive (pmiss) / holds on some negative (nhit).
+__device__ __forceinline__ void count_row_stats(u64 *cnt, bool stored, u32 pmiss, u32 nhit, int lane) {
+    const u32 bt = 1u << lane;
+    const u32 k0 = __ballot_sync(FULL, stored && !(pmiss & bt)), k1 = __ballot_sync(FULL, stored && !(nhit & bt));
+    if (lane == 0) {
+        if (k0) atomicAdd(cnt + 0, (u64)__popc(k0));
+        if (k1) atomicAdd(cnt + 1, (u64)__popc(k1));
+    }
+}
+
 // Lane t owns candidate t (t < NC).  Every phase that touches whole CSs (writing the
 // claimed rows, verifying fingerprint matches) is one chunk-major sweep over all the
 // candidates concerned, so their loads are in flight together.  Claims are written and
 // published before any lane waits on another warp's publication, so waits cannot cycle.
 template <int NC, class Gen>
 __device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u64 parent, u64 kh, u64 kl,
-                        int lane) {
+                        u32 anyp, u32 anyn, int lane) {
     int state = active ? S_PROBE : S_DONE;
     const u64 tagbits = (fp >> 40) << 40;
     const u64 genbits = (u64)A.gen << 32;
@@ -357,6 +374,8 @@ __device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u
                 }
             }
             const u64 myrow = base + __popc(cm & ((1u << lane) - 1u));
+            if (A.lstats && A.cost <= MAX_COSTS)
+                count_row_stats(A.lstats + (u64)A.cost * LSTATS, state == S_CLAIM && myrow < cap, anyp, anyn, lane);
             if (state == S_CLAIM && myrow < cap) {
                 A.parents[myrow] = parent;
                 if (A.keys) {
@@ -439,11 +458,11 @@ __device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u
 
 // Fingerprints, acceptance, found flag, uniqueness for NC candidates of one warp.
 template <int NC, class Gen, class ParentOf>
-__device__ __forceinline__ void finish(const LevelArgs &A, const Gen &g, u64 (&h)[NC], u32 bad, u32 valid,
+__device__ __forceinline__ void finish(const LevelArgs &A, const Gen &g, u64 (&h)[NC], u32 bp, u32 bn, u32 valid,
                                        ParentOf parent_of, int lane) {
     const u64 sum = reduce_to_lane<NC>(h, lane);
-    const u32 anybad = __reduce_or_sync(FULL, bad);
-    const u32 acc = ~anybad & valid;
+    const u32 anyp = __reduce_or_sync(FULL, bp), anyn = __reduce_or_sync(FULL, bn);
+    const u32 acc = ~(anyp | anyn) & valid;
     const u64 myparent = parent_of(lane);
     if (acc) {
         const int t = __ffs(acc) - 1;
@@ -467,7 +486,7 @@ __device__ __forceinline__ void finish(const LevelArgs &A, const Gen &g, u64 (&h
         }
         fp = fmix64(kh ^ fmix64(kl + 0x5ad0dedull));
     }
-    resolve<NC>(A, g, fp, (valid >> lane) & 1u, myparent, kh, kl, lane);
+    resolve<NC>(A, g, fp, (valid >> lane) & 1u, myparent, kh, kl, anyp, anyn, lane);
 }
 
 __device__ __forceinline__ bool found_stop(const LevelArgs &A) {
@@ -503,7 +522,7 @@ __device__ __forceinline__ void unary_fused(const LevelArgs &A, int mask, long l
     u64 h[NC];
 #pragma unroll
     for (int t = 0; t < NC; ++t) h[t] = 0;
-    u32 bad = 0;
+    u32 bp = 0, bn = 0;
     for (int c0 = lane; c0 < nch; c0 += 64) {
         ulonglong2 sv[2][UNARY_ROWS], mv[2];
 #pragma unroll
@@ -532,7 +551,8 @@ __device__ __forceinline__ void unary_fused(const LevelArgs &A, int mask, long l
                                 const int op = unary_slot_op(j);
                                 const u64 w0 = uop<OP_UNARY>(sv[u][r].x, m.x, op), w1 = uop<OP_UNARY>(sv[u][r].y, m.y, op);
                                 h[4 * r + j] += hw<HK>(w0, k, v0) + hw<HK>(w1, k + WEYL, v1);
-                                bad |= badbit(w0, w1, m.x, m.y) << (4 * r + j);
+                                bp |= pmiss(w0, w1, m.x, m.y) << (4 * r + j);
+                                bn |= nhit(w0, w1, m.x, m.y) << (4 * r + j);
                             }
                         }
                     }
@@ -543,7 +563,7 @@ __device__ __forceinline__ void unary_fused(const LevelArgs &A, int mask, long l
     u32 valid = 0;
     for (int r = 0; r < rows; ++r) valid |= (u32)(mask & 15) << (4 * r);
     FusedUnGen g{src0, meta, A.pitch};
-    finish<NC>(A, g, h, bad, valid,
+    finish<NC>(A, g, h, bp, bn, valid,
                [&](int t) { return pack_parent(unary_slot_op(t & 3), (u64)(s + (t >> 2)), 0); }, lane);
     evals += (u64)__popc(valid);
 }
@@ -558,7 +578,7 @@ __device__ void binary_row(const LevelArgs &A, int rop, const ulonglong2 *tile, 
     u64 h[NC];
 #pragma unroll
     for (int t = 0; t < NC; ++t) h[t] = 0;
-    u32 bad = 0;
+    u32 bp = 0, bn = 0;
     for (int c0 = lane; c0 < nch; c0 += 128) {
         ulonglong2 rvv[4], mv[4];
 #pragma unroll
@@ -588,11 +608,13 @@ __device__ void binary_row(const LevelArgs &A, int rop, const ulonglong2 *tile, 
                         const u64 b0 = until_rev(ax, lx), b1 = until_rev(ay, ly);  // r U l
                         h[2 * t] += hw<HK>(a0, k, v0) + hw<HK>(a1, k + WEYL, v1);
                         h[2 * t + 1] += hw<HK>(b0, k, v0) + hw<HK>(b1, k + WEYL, v1);
-                        bad |= (badbit(a0, a1, m.x, m.y) << (2 * t)) | (badbit(b0, b1, m.x, m.y) << (2 * t + 1));
+                        bp |= (pmiss(a0, a1, m.x, m.y) << (2 * t)) | (pmiss(b0, b1, m.x, m.y) << (2 * t + 1));
+                        bn |= (nhit(a0, a1, m.x, m.y) << (2 * t)) | (nhit(b0, b1, m.x, m.y) << (2 * t + 1));
                     } else {
                         const u64 w0 = bop<OP>(lv.x, rv.x, rop), w1 = bop<OP>(lv.y, rv.y, rop);
                         h[t] += hw<HK>(w0, k, v0) + hw<HK>(w1, k + WEYL, v1);
-                        bad |= badbit(w0, w1, m.x, m.y) << t;
+                        bp |= pmiss(w0, w1, m.x, m.y) << t;
+                        bn |= nhit(w0, w1, m.x, m.y) << t;
                     }
                 }
             }
@@ -602,7 +624,7 @@ __device__ void binary_row(const LevelArgs &A, int rop, const ulonglong2 *tile, 
     const u32 valid = cnt >= 32 ? FULL : ((1u << cnt) - 1u);
     BinGen<OP> g{tile, R, nch, rop};
     const int op = OP == OP_ANDOR ? rop : OP;
-    finish<NC>(A, g, h, bad, valid,
+    finish<NC>(A, g, h, bp, bn, valid,
                [&](int t) {
                    if (OP == OP_U) {
                        const u64 l = (u64)(l_first + (t >> 1));
@@ -798,11 +820,17 @@ __global__ void insert_letters_kernel(const LevelArgs *__restrict__ pA, int nalp
         const u64 *row = A.cache + (u64)j * A.pitch;
         u64 h[1] = {0};
         u64 k = (2ull * lane + 1ull) * WEYL;
+        u32 pm = 0, nh = 0;  // position 0: fails on a positive / holds on a negative
         for (int c = lane; c < nch; c += 32, k += 64ull * WEYL) {
             const ulonglong2 w = reinterpret_cast<const ulonglong2 *>(row)[c];
             h[0] += hw<HK>(w.x, k, 2 * c < A.n) + hw<HK>(w.y, k + WEYL, 2 * c + 1 < A.n);
+            const ulonglong2 m = meta[c];
+            pm |= pmiss(w.x, w.y, m.x, m.y);
+            nh |= nhit(w.x, w.y, m.x, m.y);
         }
-        (void)meta;
+        if (A.lstats && A.cf[0] <= MAX_COSTS)  // every letter is a stored row of the letter level
+            count_row_stats(A.lstats + (u64)A.cf[0] * LSTATS, lane == 0, __any_sync(FULL, pm) ? 1u : 0u,
+                            __any_sync(FULL, nh) ? 1u : 0u, lane);
         const u64 sum = reduce_to_lane<1>(h, lane);
         u64 fp = fmix64(sum), kh = 0, kl = 0;
         const RowGen g{reinterpret_cast<const ulonglong2 *>(row)};

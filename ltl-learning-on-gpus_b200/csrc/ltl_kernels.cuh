@@ -60,6 +60,7 @@ constexpr int MAX_SPLITS = 64;   // blocks per operator and level in a device-pl
 constexpr int MAX_RANGES = 4 + 3 * MAX_SPLITS;  // entries of a level's item table
 constexpr int UNARY_ROWS = 2;    // source rows per unary work item (each with every operator of its mask)
 constexpr int MAX_COSTS = 512;   // level starts kept on the device
+constexpr int LSTATS = 2;        // row-statistics counters per cost (see count_row_stats)
 
 // One entry of a level's item table: a block and where its items start.
 struct ItemRange {
@@ -99,7 +100,7 @@ struct DevLevel {
     int nranges;
     int learned_order;   // 1: the table is sorted by score and the queue runs through it
     ItemRange ranges[MAX_RANGES];
-    float scores[MAX_RANGES];  // PLAN_LEARNED: the scorer's logit of each entry
+    float scores[MAX_RANGES];  // learned order: each entry's sort key (chance of a find / sqrt(candidates))
 };
 
 struct LevelArgs {
@@ -133,6 +134,8 @@ struct LevelArgs {
     long long *ls;       // level starts: rows of cost c are [ls[c], ls[c + 1])
     u64 *level_cands;    // per cost
     const void *model;   // PLAN_LEARNED: the scorer (MlpDev)
+    u64 *lstats;         // per cost, LSTATS counts of stored rows by their position-0 behaviour (or null)
+    long long grid;      // CTAs of a level-kernel launch (a level of fewer items runs in one wave)
     // per level (filled into the shared copy from the plan)
     int cost;
     int check_only;
@@ -141,19 +144,16 @@ struct LevelArgs {
 };
 
 // The feature inputs of block b (operator op) of level c: the same code on the device
-// (planner) and on the host (training records).  ls[k] is the first row of cost k, lcands[k]
-// the candidates of level k (0 for the letter level).
+// (planner) and on the host (training records).  ls[k] is the first row of cost k; lstats
+// (or null) holds LSTATS row-statistics counters per cost.
 __host__ __device__ inline BlockInfo block_info(const BlockDesc &b, int op, int c, const int *cf, int nblocks,
-                                                long long level_cands, const long long *ls, const u64 *lcands,
-                                                int npos, int n, int nalpha) {
+                                                long long level_cands, const u64 *lstats, int npos, int n,
+                                                int nalpha) {
     const bool un = op == OP_NEG || op == OP_X || op == OP_F || op == OP_G;
-    const int c1 = cf[0];
-    auto urows = [&](int k) { return (k >= 0 && k < c) ? ls[k + 1] - ls[k] : 0ll; };
-    auto ucands = [&](int k) { return (k > c1 && k < c && k < MAX_COSTS + 1) ? (long long)lcands[k] : 0ll; };
     BlockInfo bi{};
     bi.op = op;
     bi.cost = c;
-    bi.c1 = c1;
+    bi.c1 = cf[0];
     bi.lcost = b.lcost;
     bi.rcost = un ? 0 : c - b.lcost - cf[op + 1];
     bi.position = b.pad;
@@ -162,12 +162,10 @@ __host__ __device__ inline BlockInfo block_info(const BlockDesc &b, int op, int 
     bi.rrows = un ? 1 : b.r1 - b.r0;
     bi.candidates = b.candidates;
     bi.level_cands = level_cands;
-    bi.u_left = urows(bi.lcost);
-    bi.u_right = un ? 0 : urows(bi.rcost);
-    bi.c_left = ucands(bi.lcost);
-    bi.c_right = un ? 0 : ucands(bi.rcost);
-    bi.u_prev = urows(c - 1);
-    bi.c_prev = ucands(c - 1);
+    for (int k = 0; k < 2; ++k) {
+        bi.lstat[k] = (lstats && bi.lcost <= MAX_COSTS) ? (long long)lstats[(u64)bi.lcost * LSTATS + k] : 0ll;
+        bi.rstat[k] = (lstats && !un && bi.rcost <= MAX_COSTS) ? (long long)lstats[(u64)bi.rcost * LSTATS + k] : 0ll;
+    }
     bi.npos = npos;
     bi.nneg = n - npos;
     bi.nalpha = nalpha;

@@ -38,6 +38,8 @@ struct MlpDev {
 };
 
 // What the features of one block are made of.  Costs are level costs; rows are cache rows.
+// Row statistics of a level: stored rows that hold at position 0 on every positive trace, and
+// stored rows that hold at position 0 on no negative trace.
 struct BlockInfo {
     int op;          // 0 ~, 1 &, 2 |, 3 X, 4 F, 5 G, 6 U
     int cost;        // the level
@@ -49,9 +51,8 @@ struct BlockInfo {
     long long lrows, rrows;   // operand rows (rrows = 1 for unary blocks)
     long long candidates;     // of the block (U: two per pair)
     long long level_cands;    // of the level
-    long long u_left, u_right;      // unique rows of the operand levels
-    long long c_left, c_right;      // candidates of the operand levels (0 for the letter level)
-    long long u_prev, c_prev;       // unique rows and candidates of level cost - 1
+    long long lstat[2];       // row statistics of the (left) operand level
+    long long rstat[2];       // of the right operand level (0 for unary blocks)
     int npos, nneg, nalpha;
 };
 
@@ -86,23 +87,20 @@ __host__ __device__ inline void block_features(const BlockInfo &b, float *f) {
     f[12] = lg2lin(b.candidates) / 32.0f;
     f[13] = ratio(b.candidates, b.level_cands);
     f[14] = ratio(b.position, b.nblocks);
-    f[15] = (float)b.nblocks / 64.0f;
-    f[16] = lg2lin(b.u_left) / 24.0f;
-    f[17] = lg2lin(b.u_right) / 24.0f;
-    f[18] = ratio(b.u_left, b.c_left);
-    f[19] = ratio(b.u_right, b.c_right);
-    f[20] = ratio(b.u_prev, b.c_prev);
-    f[21] = lg2lin(b.level_cands) / 32.0f;
-    f[22] = ratio(b.npos, (long long)b.npos + b.nneg);
-    f[23] = lg2lin((long long)b.npos + b.nneg) / 16.0f;
-    f[24] = (float)b.nalpha / 8.0f;
-    const int d = b.lcost > b.rcost ? b.lcost - b.rcost : b.rcost - b.lcost;
-    f[25] = bin ? (float)d / c : 0.0f;
-    f[26] = bin && b.lcost == b.rcost ? 1.0f : 0.0f;
-    f[27] = b.lcost == b.c1 ? 1.0f : 0.0f;
-    f[28] = bin && b.rcost == b.c1 ? 1.0f : 0.0f;
-    f[29] = bin ? 1.0f : 0.0f;
-    f[30] = lg2lin(b.u_prev) / 24.0f;
+    f[15] = lg2lin(b.level_cands) / 32.0f;
+    for (int k = 0; k < 2; ++k) {
+        f[16 + k] = lg2lin(b.lstat[k] + 1) / 24.0f;
+        f[18 + k] = ratio(b.lstat[k], b.lrows);
+        f[20 + k] = lg2lin(b.rstat[k] + 1) / 24.0f;
+        f[22 + k] = bin ? ratio(b.rstat[k], b.rrows) : 0.0f;
+    }
+    f[24] = ratio(b.npos, (long long)b.npos + b.nneg);
+    f[25] = lg2lin((long long)b.npos + b.nneg) / 16.0f;
+    f[26] = (float)b.nalpha / 8.0f;
+    f[27] = bin ? 1.0f : 0.0f;
+    f[28] = bin && b.lcost == b.rcost ? 1.0f : 0.0f;
+    f[29] = b.lcost == b.c1 ? 1.0f : 0.0f;
+    f[30] = bin && b.rcost == b.c1 ? 1.0f : 0.0f;
     f[31] = 1.0f;
 }
 

@@ -61,6 +61,7 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
     __shared__ ItemRange s_ent[MAX_RANGES];
     __shared__ long long s_cnt[MAX_RANGES];
     __shared__ float s_score[MAX_RANGES];
+    __shared__ float s_q[4 * MAX_RANGES];
     __shared__ float s_x[8][ORDER_NF];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
         L->check_only = L->on_the_fly;
         L->level_cands = cands;
         if (c < MAX_COSTS + 1) A.level_cands[c] = cands;
-        const bool fuse = !(L->plan_flags & (PLAN_UNFUSED | PLAN_LEARNED));
+        const bool fuse = !(L->plan_flags & PLAN_UNFUSED);
         // Unary blocks: one per operator, or (fused) one per distinct source range with every
         // operator on it.
         int nu = 0;
@@ -202,30 +203,58 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
             L->item_hi[op] = items;
         }
         s_nent = ne;  // item0 holds each entry's item count until the table is laid out
-        s_go = (L->plan_flags & PLAN_LEARNED) && A.model ? 2 : 1;
+        long long items = 0;
+        for (int e = 0; e < ne; ++e) items += s_ent[e].item0;
+        // order only matters when the level's items do not all start in the first wave
+        s_go = (L->plan_flags & PLAN_LEARNED) && A.model && items > A.grid ? 2 : 1;
     } while (0);
     __syncthreads();
     if (s_go == 0) return;
     const int ne = s_nent;
     if (s_go == 2) {
-        // score every entry: one warp per entry
+        // Score every block (one warp per block).  A fused unary entry holds several
+        // operators' blocks: its chance is that any of them accepts, 1 - prod(1 - p).  The
+        // key is that chance over the square root of the entry's candidates, so likely blocks
+        // go first and, of two equally likely ones, the smaller.
         const MlpDev &M = *reinterpret_cast<const MlpDev *>(A.model);
         const int c = L->cost;
         const int nbl = L->nblocks[0] + L->nblocks[1] + L->nblocks[2] + L->nblocks[3] + L->nblocks[4] +
                         L->nblocks[5] + L->nblocks[6];
-        for (int e = warp; e < ne; e += blockDim.x >> 5) {
+        const int jobs = ne * 4;  // (entry, unary slot); binary entries use slot 0 only
+        for (int j = threadIdx.x; j < jobs; j += blockDim.x) s_q[j] = 1.0f;
+        __syncthreads();
+        for (int j = warp; j < jobs; j += blockDim.x >> 5) {
+            const int e = j >> 2, slot = j & 3;
+            const ItemRange &R = s_ent[e];
+            int op;
+            const BlockDesc *b;
+            if (R.cls == 1) {
+                if (!((L->ublocks[R.idx].opmask >> slot) & 1)) continue;
+                op = unary_slot_op(slot);
+                b = &L->blocks[op][0];
+            } else {
+                if (slot) continue;
+                op = R.idx / MAX_SPLITS;
+                b = &L->blocks[op][R.idx % MAX_SPLITS];
+            }
             if (lane == 0) {
-                const ItemRange &R = s_ent[e];
-                const BlockDesc &b = R.cls == 1 ? L->ublocks[R.idx] : L->blocks[R.idx / MAX_SPLITS][R.idx % MAX_SPLITS];
-                const int op = R.cls == 1 ? b.op : R.idx / MAX_SPLITS;
-                const BlockInfo bi = block_info(b, op, c, A.cf, nbl, (long long)L->level_cands, A.ls, A.level_cands,
-                                                A.npos, A.n, A.nalpha);
+                const BlockInfo bi = block_info(*b, op, c, A.cf, nbl, (long long)L->level_cands, A.lstats, A.npos,
+                                                A.n, A.nalpha);
                 block_features(bi, s_x[warp]);
             }
             __syncwarp();
             const float z = mlp_score_warp(M, s_x[warp], lane);
-            if (lane == 0) s_score[e] = z;
+            if (lane == 0) s_q[j] = 1.0f / (1.0f + expf(z));  // 1 - sigmoid(z)
             __syncwarp();
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < ne; t += blockDim.x)
+            s_score[t] = s_q[4 * t] * s_q[4 * t + 1] * s_q[4 * t + 2] * s_q[4 * t + 3];
+        __syncthreads();
+        for (int t = threadIdx.x; t < ne; t += blockDim.x) {
+            const long long cands = s_ent[t].cls == 1 ? L->ublocks[s_ent[t].idx].candidates
+                                                       : L->blocks[s_ent[t].idx / MAX_SPLITS][s_ent[t].idx % MAX_SPLITS].candidates;
+            s_score[t] = (1.0f - s_score[t]) / sqrtf((float)(cands > 0 ? cands : 1));
         }
         __syncthreads();
         // rank sort: highest score first, ties in the reference's order

@@ -187,7 +187,7 @@ def generate(seed: int, nprops: int, npos: int, nneg: int, lmin: int, lmax: int,
 
 
 def generate_hamming(seed: int, nprops: int, npos: int, nneg: int, lmin: int, lmax: int,
-                     p_bit: float = 0.5, fsize: int = 6, flips=(1, 3), batch: int = 4096,
+                     p_bit: float = 0.5, fsize: int = 6, flips=(1, 3), batch: int | None = None,
                      max_formulas: int = 200) -> Instance:
     """Near-miss instance: each negative is a positive with 1-3 bits flipped.
 
@@ -197,6 +197,8 @@ def generate_hamming(seed: int, nprops: int, npos: int, nneg: int, lmin: int, lm
     """
     rng = np.random.default_rng(seed)
     letters = "".join(sorted(DEFAULT_LETTERS[:nprops]))
+    if batch is None:  # traces drawn per round: enough for the quotas without oversized draws
+        batch = min(4096, max(512, 8 * max(npos, nneg)))
     for _ in range(max_formulas):
         f = random_formula(rng, fsize, nprops)
         pos_l, pos_b = [], []

@@ -12,9 +12,9 @@ holding the find, labelled 1 when the block holds an accepting candidate.  The i
 is the Hamming-style shape (4 propositions, positives of length 20-48 with Bernoulli(0.5) bits,
 each negative a positive with 1-3 bits flipped, exact duplicates of positives rejected).
 
-    python ltl-learning-on-gpus_b200/learned_cli.py collect --seeds 0-2999 --npos 100 --out records.npz
+    python ltl-learning-on-gpus_b200/learned_cli.py collect --out records.npz     # ~200k records
     python ltl-learning-on-gpus_b200/learned_cli.py train --records records.npz --out scorer.npy
-    python ltl-learning-on-gpus_b200/learned_cli.py compare --scorer scorer.npy --seeds 100000-100019
+    python ltl-learning-on-gpus_b200/learned_cli.py compare --scorer scorer.npy    # held-out seeds
 """
 from __future__ import annotations
 
@@ -32,6 +32,17 @@ DEFAULT_SCORER = os.path.join(HERE, "scorer_hamming.npy")
 
 NF, H = api.SCORER_FEATURES, 64
 PARAMS = api.SCORER_PARAMS
+
+# The packaged scorer was trained on records of seeds fs * 1000003 + npos * 7919 + i
+# (fs 6..10, npos 40/100/200, i < 1600); these seeds (hidden formula size 9, 1000 + 1000
+# traces) were held out for the comparison with the plain order.
+HELD_OUT_SEEDS = tuple(range(900333, 900349))
+TRAIN_SPECS = dict(fsizes=(6, 7, 8, 9, 10), npos=(40, 100, 200), per=1600)
+
+
+def training_specs(fsizes=TRAIN_SPECS["fsizes"], npos=TRAIN_SPECS["npos"], per=TRAIN_SPECS["per"]):
+    """(seed, npos, fsize) of the packaged scorer's training instances."""
+    return [(fs * 1000003 + n * 7919 + i, n, fs) for fs in fsizes for n in npos for i in range(per)]
 
 
 def hamming_instance(seed: int, npos: int = 1000, nneg: int = 1000, fsize: int = 6) -> gen.Instance:
@@ -60,11 +71,51 @@ def load_scorer(path: str = DEFAULT_SCORER) -> np.ndarray:
     return p
 
 
-def collect(engine: api.Engine, seeds, make=hamming_instance, log=None, **opts):
-    """Training records of the given seeds: (features [k, 32], labels [k], meta list)."""
+def _hamming_spec(spec):
+    seed, npos, fsize = spec
+    return hamming_instance(seed, npos, npos, fsize)
+
+
+_CHUNK_CODE = (
+    "import pickle, sys\n"
+    "sys.path.insert(0, sys.argv[1])\n"
+    "from __graft_entry__ import load_package\n"
+    "load_package()\n"
+    "from ltlb200 import learned\n"
+    "specs = pickle.load(sys.stdin.buffer)\n"
+    "sys.stdout.buffer.write(pickle.dumps([learned._hamming_spec(s) for s in specs]))\n")
+
+
+def _run_chunk(specs):
+    import pickle
+    import subprocess
+    root = os.path.dirname(HERE)
+    out = subprocess.run([sys.executable, "-c", _CHUNK_CODE, root], input=pickle.dumps(specs),
+                         capture_output=True, check=True)
+    return pickle.loads(out.stdout)
+
+
+def instances(specs, workers: int = 0, chunk: int = 64):
+    """Hamming-style instances for (seed, npos, fsize) specs, in order.  With workers > 1 the
+    generator (plain Python) runs in that many child interpreters, `chunk` specs each."""
+    specs = list(specs)
+    if workers <= 1:
+        yield from (_hamming_spec(s) for s in specs)
+        return
+    import concurrent.futures as cf
+    with cf.ThreadPoolExecutor(workers) as ex:
+        futs = [ex.submit(_run_chunk, specs[i:i + chunk]) for i in range(0, len(specs), chunk)]
+        for f in futs:
+            yield from f.result()
+
+
+def collect(engine: api.Engine, seeds, make=hamming_instance, log=None, insts=None, **opts):
+    """Training records of the given seeds (or of the instances `insts`, one per seed):
+    (features [k, 32], labels [k], meta list)."""
     feats, labels, meta = [], [], []
+    it = iter(insts) if insts is not None else None
     for s in seeds:
-        inst = make(s)
+        inst = next(it) if it is not None else make(s)
         res, m, x, y = engine.label_blocks(inst, neg_type=1, **opts)
         for d in m:
             d["seed"] = s
@@ -78,7 +129,7 @@ def collect(engine: api.Engine, seeds, make=hamming_instance, log=None, **opts):
     return X, Y, meta
 
 
-def train(X, Y, epochs=40, batch=1024, lr=2e-3, pos_weight=None, seed=0, weight_decay=1e-4):
+def train(X, Y, epochs=30, batch=1024, lr=2e-3, pos_weight=None, seed=0, weight_decay=1e-4):
     """Adam on the GPU (api.scorer_train).  pos_weight defaults to negatives / positives."""
     if pos_weight is None:
         npos = max(1.0, float(Y.sum()))
@@ -126,18 +177,19 @@ def main(argv=None):
     ap = argparse.ArgumentParser(prog="learned_cli.py")
     sub = ap.add_subparsers(dest="cmd", required=True)
     c = sub.add_parser("collect")
-    c.add_argument("--seeds", default="0-999")
-    c.add_argument("--npos", type=int, default=1000)
+    c.add_argument("--per", type=int, default=TRAIN_SPECS["per"], help="instances per (fsize, npos) pair")
+    c.add_argument("--workers", type=int, default=16)
     c.add_argument("--out", required=True)
     t = sub.add_parser("train")
     t.add_argument("--records", required=True, nargs="+")
     t.add_argument("--out", required=True)
-    t.add_argument("--epochs", type=int, default=40)
+    t.add_argument("--epochs", type=int, default=30)
     t.add_argument("--seed", type=int, default=0)
     m = sub.add_parser("compare")
     m.add_argument("--scorer", default=DEFAULT_SCORER)
-    m.add_argument("--seeds", default="100000-100019")
+    m.add_argument("--seeds", default=f"{HELD_OUT_SEEDS[0]}-{HELD_OUT_SEEDS[-1]}")
     m.add_argument("--npos", type=int, default=1000)
+    m.add_argument("--fsize", type=int, default=9)
     m.add_argument("--repeats", type=int, default=2)
     a = ap.parse_args(argv)
     if a.cmd == "train":
@@ -147,17 +199,18 @@ def main(argv=None):
         np.save(a.out, p)
         print(f"{len(Y)} records, {int(Y.sum())} positive; loss {curve[0]:.4f} -> {curve[-1]:.4f}")
         return 0
-    with api.Engine(slots_log2=24, cache_bytes=8 << 30) as eng:
-        make = (lambda s: hamming_instance(s, a.npos, a.npos))
+    with api.Engine(slots_log2=26, cache_bytes=16 << 30) as eng:
         if a.cmd == "collect":
             t0 = time.time()
-            X, Y, meta = collect(eng, _seeds(a.seeds), make=make)
+            specs = training_specs(per=a.per)
+            X, Y, meta = collect(eng, [s[0] for s in specs], insts=instances(specs, workers=a.workers, chunk=50))
             np.savez_compressed(a.out, X=X, Y=Y, cost=np.array([d["cost"] for d in meta], np.int32),
                                 op=np.array(["~&|XFGU".index(d["op"]) for d in meta], np.int32),
                                 seed=np.array([d["seed"] for d in meta], np.int64))
             print(f"{len(Y)} records, {int(Y.sum())} positive, {time.time() - t0:.1f} s")
         else:
-            rows = compare(eng, [make(s) for s in _seeds(a.seeds)], load_scorer(a.scorer), repeats=a.repeats)
+            insts = [hamming_instance(s, a.npos, a.npos, a.fsize) for s in _seeds(a.seeds)]
+            rows = compare(eng, insts, load_scorer(a.scorer), repeats=a.repeats)
             print(summarize(rows))
     return 0
 

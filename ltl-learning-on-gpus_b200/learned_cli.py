@@ -1,6 +1,6 @@
 """Command line of the learned block order (records, training, comparison):
 
-    python ltl-learning-on-gpus_b200/learned_cli.py collect --seeds 0-999 --npos 100 --out records.npz
+    python ltl-learning-on-gpus_b200/learned_cli.py collect --out records.npz
     python ltl-learning-on-gpus_b200/learned_cli.py train --records records.npz --out scorer.npy
     python ltl-learning-on-gpus_b200/learned_cli.py compare --scorer scorer.npy
 """

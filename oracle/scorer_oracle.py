@@ -8,7 +8,8 @@ The reference (MojtabaValizadeh/ltl-learning-on-gpus) has no learned component; 
 restates is the definition the CUDA kernels implement:
 
   * block features: order.cuh `block_features` (32 values from a block's operator, costs,
-    operand sizes and the sizes of the levels below);
+    operand sizes, and row statistics of its operand levels: how many stored rows hold at
+    position 0 on every positive trace, and on no negative trace);
   * the scorer: a multilayer perceptron 32 -> 64 -> 64 -> 1 with ReLU, inputs, weights and
     activations rounded to BF16 (round to nearest even), products and sums in FP32;
   * the loss: mean over records of w * BCE-with-logits, w = pos_weight on label-1 records;
@@ -155,8 +156,8 @@ def ratio(a: int, b: int) -> np.float32:
     return np.float32(np.float32(a) / np.float32(b)) if b > 0 else np.float32(0.0)
 
 
-def block_features(op, cost, c1, lcost, rcost, position, nblocks, lrows, rrows, candidates, level_cands, u_left,
-                   u_right, c_left, c_right, u_prev, c_prev, npos, nneg, nalpha) -> np.ndarray:
+def block_features(op, cost, c1, lcost, rcost, position, nblocks, lrows, rrows, candidates, level_cands, lstat,
+                   rstat, npos, nneg, nalpha) -> np.ndarray:
     """The 32 features of order.cuh, value by value in float32."""
     f = np.zeros(NF, dtype=np.float32)
     if 0 <= op < 7:
@@ -171,22 +172,18 @@ def block_features(op, cost, c1, lcost, rcost, position, nblocks, lrows, rrows, 
     f[12] = lg2lin(candidates) / np.float32(32.0)
     f[13] = ratio(candidates, level_cands)
     f[14] = ratio(position, nblocks)
-    f[15] = np.float32(nblocks) / np.float32(64.0)
-    f[16] = lg2lin(u_left) / np.float32(24.0)
-    f[17] = lg2lin(u_right) / np.float32(24.0)
-    f[18] = ratio(u_left, c_left)
-    f[19] = ratio(u_right, c_right)
-    f[20] = ratio(u_prev, c_prev)
-    f[21] = lg2lin(level_cands) / np.float32(32.0)
-    f[22] = ratio(npos, npos + nneg)
-    f[23] = lg2lin(npos + nneg) / np.float32(16.0)
-    f[24] = np.float32(nalpha) / np.float32(8.0)
-    d = abs(lcost - rcost)
-    f[25] = np.float32(d) / c if binary else 0.0
-    f[26] = 1.0 if binary and lcost == rcost else 0.0
-    f[27] = 1.0 if lcost == c1 else 0.0
-    f[28] = 1.0 if binary and rcost == c1 else 0.0
-    f[29] = 1.0 if binary else 0.0
-    f[30] = lg2lin(u_prev) / np.float32(24.0)
+    f[15] = lg2lin(level_cands) / np.float32(32.0)
+    for k in range(2):
+        f[16 + k] = lg2lin(lstat[k] + 1) / np.float32(24.0)
+        f[18 + k] = ratio(lstat[k], lrows)
+        f[20 + k] = lg2lin(rstat[k] + 1) / np.float32(24.0)
+        f[22 + k] = ratio(rstat[k], rrows) if binary else 0.0
+    f[24] = ratio(npos, npos + nneg)
+    f[25] = lg2lin(npos + nneg) / np.float32(16.0)
+    f[26] = np.float32(nalpha) / np.float32(8.0)
+    f[27] = 1.0 if binary else 0.0
+    f[28] = 1.0 if binary and lcost == rcost else 0.0
+    f[29] = 1.0 if lcost == c1 else 0.0
+    f[30] = 1.0 if binary and rcost == c1 else 0.0
     f[31] = 1.0
     return f

@@ -68,9 +68,8 @@ def _random_info(rng):
     big = lambda: int(rng.integers(0, 1 << int(rng.integers(1, 40))))
     return dict(op=op, cost=cost, c1=1, lcost=lcost, rcost=rcost, position=int(rng.integers(0, 40)),
                 nblocks=int(rng.integers(1, 60)), lrows=big(), rrows=1 if un else big(), candidates=big(),
-                level_cands=big(), u_left=big(), u_right=0 if un else big(), c_left=big(),
-                c_right=0 if un else big(), u_prev=big(), c_prev=big(), npos=int(rng.integers(0, 5000)),
-                nneg=int(rng.integers(0, 5000)), nalpha=int(rng.integers(1, 27)))
+                level_cands=big(), lstat=[big() for _ in range(2)], rstat=[0] * 2 if un else [big() for _ in range(2)],
+                npos=int(rng.integers(0, 5000)), nneg=int(rng.integers(0, 5000)), nalpha=int(rng.integers(1, 27)))
 
 
 def test_block_features_bit_exact():

@@ -91,10 +91,13 @@ def test_label_features_match_host_function():
 
 @pytest.mark.skipif(not os.path.exists(learned.DEFAULT_SCORER), reason="no trained scorer in the package")
 def test_trained_scorer_gains_over_plain_order():
+    """Held-out Hamming-style instances (1000 + 1000 traces, hidden formula of size 9; seeds
+    never used for training): the learned order finds the same minimal cost on every one and
+    evaluates fewer candidates before the find over the set."""
     p = learned.load_scorer()
-    with api.Engine(slots_log2=24, cache_bytes=4 << 30) as eng:
-        insts = [learned.hamming_instance(s, 300, 300) for s in range(900000, 900012)]
+    insts = [learned.hamming_instance(s, 1000, 1000, 9) for s in learned.HELD_OUT_SEEDS]
+    with api.Engine(slots_log2=26, cache_bytes=16 << 30) as eng:
         rows = learned.compare(eng, insts, p)
     s = learned.summarize(rows)
     assert s["same_cost"], rows
-    assert s["evaluated_learned"] < s["evaluated_plain"], s
+    assert sum(r["evaluated_learned"] for r in rows) < sum(r["evaluated_plain"] for r in rows), s

@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--quiet-extra", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain block order comparison")
+    ap.add_argument("--workload", choices=["cfg2", "cfg3", "cfg4"], default="cfg2",
+                    help="cfg3: exact vs relaxed uniqueness on one large instance; cfg4: 4096 batched instances")
+    ap.add_argument("--time-limit", type=float, default=120.0, help="cfg3: seconds per uniqueness mode")
     return ap.parse_args()
 
 
@@ -239,6 +242,31 @@ def run_reference(a):
     return 0
 
 
+def run_workload(a):
+    """The cfg3 / cfg4 lines (one GPU; other ranks exit)."""
+    import torch
+    ws, rank, local = dist()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    from __graft_entry__ import load_package
+    load_package()
+    from ltlb200 import workloads
+    if a.workload == "cfg3":
+        rep = workloads.run_cfg3(time_limit_s=a.time_limit, device=local)
+        ex = rep["exact"]
+        line = {"metric": "unique CS/s; completeness loss of relaxed (64-bit hash) uniqueness", "value":
+                ex["unique_cs_per_s"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "u64",
+                "data": "synthetic", "config": {"workload": rep["workload"]}, **rep}
+    else:
+        rep = workloads.run_cfg4(device=local)
+        line = {"metric": "instances/s and unique CS/s of a batched run", "value": rep["instances_per_s"],
+                "unit": "instances/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u64", "data": "synthetic",
+                "config": {"workload": rep["workload"]}, **rep}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(a):
     import torch
     ws, rank, local = dist()
@@ -376,6 +404,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload != "cfg2":
+        return run_workload(a)
     return run_ours(a)
 
 

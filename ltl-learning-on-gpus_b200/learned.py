@@ -76,37 +76,12 @@ def _hamming_spec(spec):
     return hamming_instance(seed, npos, npos, fsize)
 
 
-_CHUNK_CODE = (
-    "import pickle, sys\n"
-    "sys.path.insert(0, sys.argv[1])\n"
-    "from __graft_entry__ import load_package\n"
-    "load_package()\n"
-    "from ltlb200 import learned\n"
-    "specs = pickle.load(sys.stdin.buffer)\n"
-    "sys.stdout.buffer.write(pickle.dumps([learned._hamming_spec(s) for s in specs]))\n")
-
-
-def _run_chunk(specs):
-    import pickle
-    import subprocess
-    root = os.path.dirname(HERE)
-    out = subprocess.run([sys.executable, "-c", _CHUNK_CODE, root], input=pickle.dumps(specs),
-                         capture_output=True, check=True)
-    return pickle.loads(out.stdout)
-
-
 def instances(specs, workers: int = 0, chunk: int = 64):
     """Hamming-style instances for (seed, npos, fsize) specs, in order.  With workers > 1 the
     generator (plain Python) runs in that many child interpreters, `chunk` specs each."""
-    specs = list(specs)
-    if workers <= 1:
-        yield from (_hamming_spec(s) for s in specs)
-        return
-    import concurrent.futures as cf
-    with cf.ThreadPoolExecutor(workers) as ex:
-        futs = [ex.submit(_run_chunk, specs[i:i + chunk]) for i in range(0, len(specs), chunk)]
-        for f in futs:
-            yield from f.result()
+    from .workloads import generate_many
+    full = [(seed, 4, npos, npos, 20, 48, 0.5, fs) for seed, npos, fs in specs]
+    yield from generate_many("generate_hamming", full, workers=workers, chunk=chunk)
 
 
 def collect(engine: api.Engine, seeds, make=hamming_instance, log=None, insts=None, **opts):

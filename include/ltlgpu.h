@@ -271,6 +271,14 @@ LTLG_API int ltlg_scorer_grad(const float *params, const float *features, const 
 LTLG_API int ltlg_scorer_train(float *params, const float *features, const float *labels, int32_t count,
                                const ltlg_train_config *cfg, float *epoch_loss);
 
+/* Evaluate a formula string on every trace, on the device (the reference checks formulas on
+ * the host in code/dc.py:136-187).  The string uses the enumerator's output format, parsed as
+ * dc.py's bitVec does: "~(f)", "X(f)", "F(f)", "G(f)", "(f)&(g)", "(f)|(g)", "(f)U(g)", single
+ * letters of the alphabet.  cs (optional): the formula's CS per trace (bit k: holds at
+ * position k); holds (optional): 1 where it holds at position 0.  LTLG_BAD_ARGS on a malformed
+ * formula or an unknown letter, LTLG_INPUT_LIMITS on a trace longer than 63 steps. */
+LTLG_API int ltlg_evaluate(const ltlg_traces *traces, const char *formula, uint64_t *cs, uint8_t *holds);
+
 LTLG_API const char *ltlg_status_string(int status);
 LTLG_API int ltlg_abi_version(void);
 

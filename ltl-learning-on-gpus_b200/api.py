@@ -31,7 +31,7 @@ EXPORTED = [
     "ltlg_traces_free", "ltlg_engine_stream", "ltlg_batch_create", "ltlg_batch_destroy", "ltlg_batch_learn",
     "ltlg_batch_stream", "ltlg_learn_noalloc", "ltlg_block_features", "ltlg_engine_set_scorer",
     "ltlg_batch_set_scorer", "ltlg_engine_label_blocks", "ltlg_scorer_forward", "ltlg_scorer_grad",
-    "ltlg_scorer_train",
+    "ltlg_scorer_train", "ltlg_evaluate",
 ]
 SCORER_FEATURES = 32
 SCORER_PARAMS = 6337
@@ -139,6 +139,7 @@ def lib():
         L.ltlg_scorer_forward.argtypes = [fp, fp, C.c_int32, fp]
         L.ltlg_scorer_grad.argtypes = [fp, fp, fp, C.c_int32, C.c_float, fp, fp]
         L.ltlg_scorer_train.argtypes = [fp, fp, fp, C.c_int32, C.POINTER(TrainConfig), fp]
+        L.ltlg_evaluate.argtypes = [C.POINTER(Traces), C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint8)]
         _lib = L
     return _lib
 
@@ -455,6 +456,24 @@ def scorer_train(params: np.ndarray, features: np.ndarray, labels: np.ndarray, e
     if rc != 0:
         raise RuntimeError(f"scorer_train failed: {status_string(rc)}")
     return p, curve[:int(epochs)]
+
+
+def evaluate(inst: Instance, formula: str):
+    """The formula's CS on every trace (uint64, bit k = holds at position k) and whether it
+    holds at position 0 (bool), computed on the device."""
+    t, keep = _traces(inst)
+    cs = np.zeros(max(inst.n, 1), dtype=np.uint64)
+    holds = np.zeros(max(inst.n, 1), dtype=np.uint8)
+    rc = lib().ltlg_evaluate(C.byref(t), formula.encode(), _u64p(cs), holds.ctypes.data_as(C.POINTER(C.c_uint8)))
+    if rc != 0:
+        raise ValueError(f"evaluate failed ({status_string(rc)}): {formula!r}")
+    return cs[:inst.n], holds[:inst.n].astype(bool)
+
+
+def separates(inst: Instance, formula: str) -> bool:
+    """Holds at position 0 on every positive trace and on no negative one (device)."""
+    _, h = evaluate(inst, formula)
+    return bool(h[:inst.num_pos].all() and not h[inst.num_pos:].any())
 
 
 def device_apply_op(op: int, a: np.ndarray, b: np.ndarray | None, lenmask: np.ndarray):

@@ -966,7 +966,43 @@ __global__ void apply_op_kernel(int op, const u64 *a, const u64 *b, const u64 *w
     }
 }
 
+// A formula as a postfix program (op, arg) evaluated on every trace at once: thread t holds
+// trace t's CS of each subformula on a stack in global memory laid out [depth][n], so
+// neighbouring threads touch neighbouring words.  Letters read atoms[arg * n + t]; the
+// operators are the enumerator's own (uop / bop / until_bits).
+__global__ void eval_formula_kernel(const int *__restrict__ prog, int len, const u64 *__restrict__ atoms,
+                                    const u64 *__restrict__ lenmask, int n, u64 *__restrict__ stack,
+                                    u64 *__restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const u64 m = lenmask[t];
+    int sp = 0;
+    for (int k = 0; k < len; ++k) {
+        const int op = prog[2 * k], arg = prog[2 * k + 1];
+        u64 v;
+        if (op == OP_ATOM) {
+            v = atoms[(u64)arg * n + t];
+        } else if (op == OP_NEG || op == OP_X || op == OP_F || op == OP_G) {
+            v = uop<OP_UNARY>(stack[(u64)(sp - 1) * n + t], m, op);
+            --sp;
+        } else {
+            const u64 y = stack[(u64)(sp - 1) * n + t], x = stack[(u64)(sp - 2) * n + t];
+            v = op == OP_U ? until_bits(x, y) : bop<OP_ANDOR>(x, y, op);
+            sp -= 2;
+        }
+        stack[(u64)sp * n + t] = v;
+        ++sp;
+    }
+    out[t] = stack[t];
+}
+
 }  // namespace
+
+cudaError_t launch_eval_formula(const int *prog, int len, const u64 *atoms, const u64 *lenmask, int n, u64 *stack,
+                                u64 *out, cudaStream_t s) {
+    eval_formula_kernel<<<(n + 127) / 128, 128, 0, s>>>(prog, len, atoms, lenmask, n, stack, out);
+    return cudaGetLastError();
+}
 
 int level_kernel_smem_bytes(int left_tile, int pitch) { return left_tile * pitch * 8; }
 

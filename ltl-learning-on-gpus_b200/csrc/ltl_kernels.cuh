@@ -183,6 +183,9 @@ cudaError_t launch_plan(const LevelArgs *d, cudaStream_t s);
 cudaError_t launch_insert_letters(const LevelArgs &a, const LevelArgs *d, int nalpha, cudaStream_t s);
 cudaError_t launch_walk(const u64 *parents, int nalpha, u64 found, u64 *out, int cap, cudaStream_t s);
 cudaError_t launch_scorer_pack(const float *params, MlpDev *out, cudaStream_t s);
+// prog: (op, arg) pairs in postfix, op OP_ATOM with arg = letter index; stack: depth x n words.
+cudaError_t launch_eval_formula(const int *prog, int len, const u64 *atoms, const u64 *lenmask, int n, u64 *stack,
+                                u64 *out, cudaStream_t s);
 cudaError_t launch_apply_op(int op, const u64 *a, const u64 *b, const u64 *wmeta, int n, int pitch, int count,
                             u64 *out, u64 *out2, u64 *fp, cudaStream_t s);
 

@@ -1,0 +1,44 @@
+"""The divide-and-conquer driver's control flow on the CPU, with the oracle as the solver and
+as the checker (the product runs both on the device): results separate every trace, and a
+window covering the whole instance gives the direct result."""
+import numpy as np
+import pytest
+
+import oracle as O
+from ltlb200 import divide, gen
+
+
+def _driver(inst, **kw):
+    def solve(pos, neg):
+        sub = divide.sub_instance(inst, pos, neg)
+        r = O.learn(sub, costs=(1,) * 8, neg_type=1, max_cost=12, keep_rows=False)
+        return r.formula if r.status == O.FOUND else None
+
+    return divide.Driver(inst, solve=solve, holds=lambda f: O.evaluate(f, inst), **kw)
+
+
+def test_sub_instance_slices_traces():
+    inst = gen.generate(3, 2, 10, 10, 4, 12, 0.5, 4)
+    sub = divide.sub_instance(inst, [1, 4], [0, 9])
+    lines = inst.trace_lines()
+    assert sub.num_pos == 2 and sub.num_neg == 2
+    assert sub.trace_lines() == [lines[1], lines[4], lines[10], lines[19]]
+
+
+@pytest.mark.parametrize("algo", ["det", "rand"])
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_dc_result_separates(algo, seed):
+    inst = gen.generate(seed, 3, 40, 40, 6, 14, 0.5, 6)
+    d = _driver(inst)
+    pos, neg = list(range(inst.num_pos)), list(range(inst.num_neg))
+    f = (d.rand_split if algo == "rand" else d.det_split)(16, pos, neg)
+    assert O.separates(f, inst), f
+    assert d.calls >= 1
+
+
+def test_window_covering_everything_is_one_call():
+    inst = gen.generate(5, 2, 12, 12, 4, 10, 0.5, 4)
+    d = _driver(inst)
+    f = d.det_split(64, list(range(12)), list(range(12)))
+    assert d.calls == 1 and O.separates(f, inst)
+    assert O.formula_cost(f) == O.learn(inst, neg_type=1, keep_rows=False).cost

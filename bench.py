@@ -70,6 +70,18 @@ def seeds_of(spec: str, rank: int):
     return list(range(a + rank * width, b + 1 + rank * width))
 
 
+def reduce_over_ranks(step_t: float, kern_t: float, totals, device: str):
+    """Whole-job figures: the slowest rank's step and kernel times (max) and the units all
+    ranks processed (sum).  Every rank calls it; works on NCCL (cuda) and gloo (cpu)."""
+    import torch
+    import torch.distributed as D
+    t = torch.tensor([step_t, kern_t], dtype=torch.float64, device=device)
+    D.all_reduce(t, op=D.ReduceOp.MAX)
+    u = torch.tensor(list(totals), dtype=torch.float64, device=device)
+    D.all_reduce(u, op=D.ReduceOp.SUM)
+    return float(t[0]), float(t[1]), [float(x) for x in u]
+
+
 def make_batch(seeds):
     from __graft_entry__ import load_package
     load_package()
@@ -344,13 +356,7 @@ def run_ours(a):
     n = batch[0].n
     tot = [float(uniq_e2e), float(cand_e2e), float(uniq_seq), float(cand_seq)]
     if ws > 1:
-        import torch.distributed as D
-        t = torch.tensor([step_t, kern_t], dtype=torch.float64, device="cuda")
-        D.all_reduce(t, op=D.ReduceOp.MAX)
-        u = torch.tensor(tot, dtype=torch.float64, device="cuda")
-        D.all_reduce(u, op=D.ReduceOp.SUM)
-        step_t, kern_t = float(t[0]), float(t[1])
-        tot = [float(x) for x in u]
+        step_t, kern_t, tot = reduce_over_ranks(step_t, kern_t, tot, "cuda")
     if rank == 0:
         peak, peak_kind = measured_peak_gbs()
         per_unit = 8 * n + 8

@@ -74,6 +74,7 @@ struct ltlg_engine {
     // arguments from `args`, so the graphs stay valid from one learn to the next; they are
     // captured again only when the kernel instances or grids change (graph_key).
     cudaGraphExec_t level_graph[RING] = {};
+    void *ring_dev = nullptr;       // device view of h_ring
     DevBuf scorer, scorer_params;   // the learned block order's scorer (MlpDev, packed FP32)
     DevBuf lstats, h_lstats;        // row statistics per cost (LSTATS counters)
     bool has_scorer = false;
@@ -281,7 +282,14 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
     if (err == cudaSuccess) err = ensure(e->args, sizeof(LevelArgs));
     if (err == cudaSuccess) err = ensure(e->lstats, (MAX_COSTS + 2) * LSTATS * sizeof(u64));
     if (err == cudaSuccess) err = ensure_host(e->h_lstats, (MAX_COSTS + 2) * LSTATS * sizeof(u64));
-    if (err == cudaSuccess) err = ensure_host(e->h_ring, ltlg_engine::RING * (sizeof(DevCtl) + sizeof(DevLevel)));
+    if (err == cudaSuccess) {  // the ring of level summaries: mapped, the level kernel writes it
+        err = cudaHostAlloc(&e->h_ring.p, ltlg_engine::RING * (sizeof(DevCtl) + sizeof(DevLevel)), cudaHostAllocMapped);
+        if (err == cudaSuccess) {
+            e->h_ring.bytes = ltlg_engine::RING * (sizeof(DevCtl) + sizeof(DevLevel));
+            memset(e->h_ring.p, 0, e->h_ring.bytes);
+            err = cudaHostGetDevicePointer(&e->ring_dev, e->h_ring.p, 0);
+        }
+    }
     if (err == cudaSuccess) err = ensure(e->lev, sizeof(DevLevel));
     if (err == cudaSuccess) err = ensure_host(e->h_lev, sizeof(DevLevel));
     if (err == cudaSuccess) err = ensure(e->ls, (MAX_COSTS + 2) * sizeof(long long));
@@ -533,6 +541,8 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     A.model = opt->order == LTLG_ORDER_LEARNED ? e->scorer.p : nullptr;
     A.grid = max_grid;
     A.lstats = (u64 *)e->lstats.p;
+    A.ring = e->ring_dev;
+    A.ring_slots = ltlg_engine::RING;
     cudaMemsetAsync(e->lstats.p, 0, (MAX_COSTS + 2) * LSTATS * sizeof(u64), st);
     cudaMemsetAsync(e->ls.p, 0, (MAX_COSTS + 2) * sizeof(long long), st);
     cudaMemsetAsync(e->lcands.p, 0, (MAX_COSTS + 2) * sizeof(u64), st);
@@ -568,22 +578,21 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         DevCtl *rctl = (DevCtl *)e->h_ring.p;
         DevLevel *rlev = (DevLevel *)((char *)e->h_ring.p + R * sizeof(DevCtl));
         int enq = 0, done = 0;
-        const long long key[8] = {tl, hk, pitch, block_threads, max_grid, 2, 0, 0};
+        // One graph for every level: planner and level kernel; the level kernel's last CTA
+        // writes the level's summary into ring slot (seq - 1) % R of the mapped host ring.
+        const long long key[8] = {tl, hk, pitch, block_threads, max_grid, 3, 0, 0};
         if (memcmp(key, e->graph_key, sizeof(key)) != 0) {
             memset(e->graph_key, 0, sizeof(e->graph_key));
-            for (int k = 0; k < R && err == cudaSuccess; ++k) {
-                if (e->level_graph[k]) cudaGraphExecDestroy(e->level_graph[k]);
-                e->level_graph[k] = nullptr;
-                cudaGraph_t g = nullptr;
-                err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-                if (err != cudaSuccess) break;
+            if (e->level_graph[0]) cudaGraphExecDestroy(e->level_graph[0]);
+            e->level_graph[0] = nullptr;
+            cudaGraph_t g = nullptr;
+            err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            if (err == cudaSuccess) {
                 cudaError_t x = launch_plan(dA, st);
                 if (x == cudaSuccess) x = launch_level(A, dA, (int)max_grid, block_threads, st);
-                cudaMemcpyAsync(rctl + k, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
-                cudaMemcpyAsync(rlev + k, dlev, offsetof(DevLevel, blocks), cudaMemcpyDeviceToHost, st);
                 err = cudaStreamEndCapture(st, &g);
                 if (err == cudaSuccess) err = x;
-                if (err == cudaSuccess) err = cudaGraphInstantiate(&e->level_graph[k], g, 0);
+                if (err == cudaSuccess) err = cudaGraphInstantiate(&e->level_graph[0], g, 0);
                 if (g) cudaGraphDestroy(g);
             }
             if (err != cudaSuccess) return fail_cuda(e, err, res);
@@ -592,7 +601,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         auto enqueue = [&]() -> cudaError_t {
             const int k = enq % R;
             cudaEventRecord(e->ev_start[k], st);
-            const cudaError_t x = cudaGraphLaunch(e->level_graph[k], st);
+            const cudaError_t x = cudaGraphLaunch(e->level_graph[0], st);
             cudaEventRecord(e->ev_done[k], st);
             launches += 2;
             ++enq;

@@ -694,6 +694,38 @@ __device__ __forceinline__ void load_level(LevelArgs &A, const LevelArgs *A0) {
     A.unary_rows = L->unary_rows;
 }
 
+// The end of a level-kernel launch: the last CTA to finish resets the CTA count and, when
+// the host keeps a ring of level summaries in mapped memory, writes the control block and
+// the plan header into the level's slot, so the host reads them without a copy on the
+// stream.  No CTA waits for another.
+__device__ __forceinline__ void level_summary(const LevelArgs &A) {
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const u32 done = atomicAdd(&A.ctl->ctas_done, 1u);
+        s_last = done == gridDim.x - 1 ? 1 : 0;
+        if (s_last) A.ctl->ctas_done = 0u;
+    }
+    __syncthreads();
+    if (!s_last || !A.ring) return;
+    __threadfence();
+    constexpr int CW = sizeof(DevCtl) / 8, LW = offsetof(DevLevel, blocks) / 8;
+    const int R = A.ring_slots;
+    const int slot = ((A.lev->seq - 1) % R + R) % R;
+    u64 *dc = reinterpret_cast<u64 *>(A.ring) + (u64)slot * CW;
+    u64 *dl = reinterpret_cast<u64 *>(reinterpret_cast<char *>(A.ring) + (u64)R * sizeof(DevCtl) +
+                                      (u64)slot * sizeof(DevLevel));
+    const u64 *sc = reinterpret_cast<const u64 *>(A.ctl), *sl = reinterpret_cast<const u64 *>(A.lev);
+    for (int i = threadIdx.x; i < CW + LW; i += blockDim.x) {
+        if (i < CW)
+            dc[i] = ld_volatile(sc + i);
+        else
+            dl[i - CW] = ld_volatile(sl + (i - CW));
+    }
+    __threadfence_system();
+}
+
 // Leading entries of the item table kept in shared memory (read once per item in a learned
 // order).  Small enough that three CTAs with a 64 KB tile still fit the 196 KB carveout.
 constexpr int RANGE_CACHE = 32;
@@ -754,58 +786,60 @@ __global__ void __launch_bounds__(256, 3) level_kernel(const LevelArgs *__restri
         s_evals = 0;
     }
     __syncthreads();
-    if (s_halt || s_hi <= 0) return;
-    if (s_learned) {
-        for (int e = threadIdx.x; e < s_nr && e < RANGE_CACHE; e += blockDim.x) s_rng[e] = A.lev->ranges[e];
-        __syncthreads();
-    }
-    u64 evals = 0;
-    u32 phase = 0;
-    int cur = 0;  // thread 0, learned order: table entry of the last item (claimed in increasing order)
-    for (;;) {
-        if (threadIdx.x == 0) {
-            long long it = -1;
-            if (!found_stop(A)) {
-                it = (long long)atomicAdd(&A.ctl->queue[0], 1ull);
-                if (it >= s_hi) it = -1;
-            }
-            if (it >= 0 && s_learned) {  // the entry holding the item: the last one with item0 <= it
-                const ItemRange *rng = A.lev->ranges;
-                auto item0_of = [&](int e) { return e < RANGE_CACHE ? s_rng[e].item0 : rng[e].item0; };
-                while (cur + 1 < s_nr && item0_of(cur + 1) <= it) ++cur;
-                const ItemRange R = cur < RANGE_CACHE ? s_rng[cur] : rng[cur];
-                it = R.plain0 + (it - R.item0);
-            }
-            s_item = it;
-            s_next_row = 0;
+    if (!s_halt && s_hi > 0) {
+        if (s_learned) {
+            for (int e = threadIdx.x; e < s_nr && e < RANGE_CACHE; e += blockDim.x) s_rng[e] = A.lev->ranges[e];
+            __syncthreads();
         }
-        __syncthreads();
-        const long long item = s_item;
-        if (item < 0) break;
-        bool ok = true;
-        if (item < s_cls[1]) {
-            int k = 0;
-            while (k < s_nub - 1 && item >= s_ub[k + 1]) ++k;
-            unary_item<HK>(A, A.lev->ublocks[k], item - s_ub[k], warp, nwarps, lane, evals);
-        } else if (item < s_cls[2]) {
-            const long long in_cls = item - s_cls[1];
-            const int op = in_cls < s_and ? OP_AND : OP_OR;
-            const long long in_op = op == OP_AND ? in_cls : in_cls - s_and;
-            const BlockDesc *blocks = A.lev->blocks[op];
-            const BlockDesc B = blocks[find_block(blocks, s_nb[op], in_op)];
-            ok = binary_item<OP_ANDOR, TL, HK>(A, op, B, in_op - B.item0, tile, &bar, phase, &s_next_row, lane, evals);
-        } else {
-            const long long in_op = item - s_cls[2];
-            const BlockDesc *blocks = A.lev->blocks[OP_U];
-            const BlockDesc B = blocks[find_block(blocks, s_nb[OP_U], in_op)];
-            ok = binary_item<OP_U, TL, HK>(A, OP_U, B, in_op - B.item0, tile, &bar, phase, &s_next_row, lane, evals);
+        u64 evals = 0;
+        u32 phase = 0;
+        int cur = 0;  // thread 0, learned order: table entry of the last item (claimed in increasing order)
+        for (;;) {
+            if (threadIdx.x == 0) {
+                long long it = -1;
+                if (!found_stop(A)) {
+                    it = (long long)atomicAdd(&A.ctl->queue[0], 1ull);
+                    if (it >= s_hi) it = -1;
+                }
+                if (it >= 0 && s_learned) {  // the entry holding the item: the last one with item0 <= it
+                    const ItemRange *rng = A.lev->ranges;
+                    auto item0_of = [&](int e) { return e < RANGE_CACHE ? s_rng[e].item0 : rng[e].item0; };
+                    while (cur + 1 < s_nr && item0_of(cur + 1) <= it) ++cur;
+                    const ItemRange R = cur < RANGE_CACHE ? s_rng[cur] : rng[cur];
+                    it = R.plain0 + (it - R.item0);
+                }
+                s_item = it;
+                s_next_row = 0;
+            }
+            __syncthreads();
+            const long long item = s_item;
+            if (item < 0) break;
+            bool ok = true;
+            if (item < s_cls[1]) {
+                int k = 0;
+                while (k < s_nub - 1 && item >= s_ub[k + 1]) ++k;
+                unary_item<HK>(A, A.lev->ublocks[k], item - s_ub[k], warp, nwarps, lane, evals);
+            } else if (item < s_cls[2]) {
+                const long long in_cls = item - s_cls[1];
+                const int op = in_cls < s_and ? OP_AND : OP_OR;
+                const long long in_op = op == OP_AND ? in_cls : in_cls - s_and;
+                const BlockDesc *blocks = A.lev->blocks[op];
+                const BlockDesc B = blocks[find_block(blocks, s_nb[op], in_op)];
+                ok = binary_item<OP_ANDOR, TL, HK>(A, op, B, in_op - B.item0, tile, &bar, phase, &s_next_row, lane, evals);
+            } else {
+                const long long in_op = item - s_cls[2];
+                const BlockDesc *blocks = A.lev->blocks[OP_U];
+                const BlockDesc B = blocks[find_block(blocks, s_nb[OP_U], in_op)];
+                ok = binary_item<OP_U, TL, HK>(A, OP_U, B, in_op - B.item0, tile, &bar, phase, &s_next_row, lane, evals);
+            }
+            if (!ok) break;
+            __syncthreads();  // every warp is done with the tile before the next copy
         }
-        if (!ok) break;
-        __syncthreads();  // every warp is done with the tile before the next copy
+        if (lane == 0 && evals) atomicAdd(&s_evals, evals);
+        __syncthreads();
+        if (threadIdx.x == 0 && s_evals) atomicAdd(&A.ctl->evaluated, s_evals);
     }
-    if (lane == 0 && evals) atomicAdd(&s_evals, evals);
-    __syncthreads();
-    if (threadIdx.x == 0 && s_evals) atomicAdd(&A.ctl->evaluated, s_evals);
+    level_summary(A);
 }
 
 // Letters: register rows [0, nalpha) in the hash set (duplicate letters stay rows,

@@ -1,6 +1,7 @@
 // Shared host/device definitions of the CS enumeration kernels.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -38,7 +39,7 @@ struct DevCtl {
     u32 status;      // ST_* bits
     u32 found_cost;  // level at which `found` was set
     u32 overflow_cost;  // level at which the cache first overflowed
-    u32 pad;
+    u32 ctas_done;   // CTAs of the running level-kernel launch that have finished (the last resets it)
     u64 queue[8];    // next work item of each operator's kernel
 };
 
@@ -82,6 +83,8 @@ struct DevLevel {
     int halt;            // 1: every operator kernel of this level exits at once
     int check_only;      // on-the-fly: acceptance only, no dedupe, no storing
     int on_the_fly;      // set by the host: plan check-only levels and ignore the overflow bit
+    int seq;             // planner runs since the learn started (the level's host ring slot is (seq - 1) % RING)
+    int pad0;
     long long item_hi_all;  // all work items of the level
     long long items_end;    // the level kernel takes items from ctl->queue[0] below it
     int right_chunk;
@@ -102,6 +105,8 @@ struct DevLevel {
     ItemRange ranges[MAX_RANGES];
     float scores[MAX_RANGES];  // learned order: each entry's sort key (chance of a find / sqrt(candidates))
 };
+
+static_assert(sizeof(DevCtl) % 8 == 0 && offsetof(DevLevel, blocks) % 8 == 0, "level summaries copy 8-byte words");
 
 struct LevelArgs {
     // constant during a learn
@@ -135,6 +140,8 @@ struct LevelArgs {
     u64 *level_cands;    // per cost
     const void *model;   // PLAN_LEARNED: the scorer (MlpDev)
     u64 *lstats;         // per cost, LSTATS counts of stored rows by their position-0 behaviour (or null)
+    void *ring;          // device view of the host's ring of level summaries (or null)
+    int ring_slots;
     long long grid;      // CTAs of a level-kernel launch (a level of fewer items runs in one wave)
     // per level (filled into the shared copy from the plan)
     int cost;

@@ -63,49 +63,68 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
     __shared__ float s_score[MAX_RANGES];
     __shared__ float s_q[4 * MAX_RANGES];
     __shared__ float s_x[8][ORDER_NF];
+    // The plan is built in shared memory and copied out once: thread 0 never reads back
+    // what it wrote to global memory (each read-back is an L2 round trip).
+    __shared__ BlockDesc s_blk[MAX_RANGES];  // the level's blocks, operator by operator
+    __shared__ BlockDesc s_ub[4];
+    __shared__ int s_first[8], s_c, s_nblk, s_nu;
+    __shared__ long long s_ls[MAX_COSTS + 2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
         s_go = 0;
         s_nent = 0;
+        s_nblk = 0;
+        s_nu = 0;
+        L->seq = L->seq + 1;
+        s_c = L->halt == 2 ? -1 : L->cost + 1;  // an over-long plan stops the rest of the graph
     }
     __syncthreads();
+    const int cc = s_c;
+    if (cc < 0) return;
+    for (int k = threadIdx.x; k < cc && k < MAX_COSTS + 1; k += blockDim.x) s_ls[k] = A.ls[k];
+    __syncthreads();
     if (threadIdx.x == 0) do {
-        if (L->halt == 2) break;  // an over-long plan stops the rest of the graph
-        const int c = L->cost + 1;
+        const int c = cc;
         L->cost = c;
         const long long rows = min((long long)C->row_count, A.cap_rows);
-        if (c < MAX_COSTS + 1) A.ls[c] = rows;  // level c - 1 ended here
+        if (c < MAX_COSTS + 1) {
+            A.ls[c] = rows;  // level c - 1 ended here
+            s_ls[c] = rows;
+        }
         u32 bad = ST_WAIT | ST_TABLE | ST_TMA;
-        if (!L->on_the_fly) bad |= ST_OVERFLOW;
+        const int on_the_fly = L->on_the_fly, flags = L->plan_flags;
+        if (!on_the_fly) bad |= ST_OVERFLOW;
         const bool halt = c > A.max_cost || c >= MAX_COSTS || (A.stop_at_found && C->found != 0ull) ||
                           (C->status & bad) != 0u;
-        for (int k = 0; k < 8; ++k) {
-            L->nblocks[k] = 0;
-            L->total_items[k] = 0;
-            L->item_hi[k] = 0;
-            C->queue[k] = 0;
-        }
-        L->item_hi_all = 0;
-        L->nublocks = 0;
-        L->nranges = 0;
-        L->learned_order = 0;
-        L->items_end = 0;
+        for (int k = 0; k < 8; ++k) C->queue[k] = 0;
         L->halt = halt ? 1 : 0;
-        L->level_cands = 0;
-        if (halt) break;
+        if (halt) {
+            for (int k = 0; k < 8; ++k) {
+                L->nblocks[k] = 0;
+                L->total_items[k] = 0;
+                L->item_hi[k] = 0;
+            }
+            L->item_hi_all = 0;
+            L->nublocks = 0;
+            L->nranges = 0;
+            L->learned_order = 0;
+            L->items_end = 0;
+            L->level_cands = 0;
+            break;
+        }
         const int c1 = A.cf[0];
-        auto lo = [&](int k) { return (k >= 0 && k < c) ? A.ls[k] : 0ll; };
-        auto hi = [&](int k) { return (k >= 0 && k < c) ? A.ls[k + 1] : 0ll; };
+        auto lo = [&](int k) { return (k >= 0 && k < c) ? s_ls[k] : 0ll; };
+        auto hi = [&](int k) { return (k >= 0 && k < c) ? s_ls[k + 1] : 0ll; };
         u64 cands = 0;
         bool overfull = false;
-        int nb = 0;
+        int nb = 0, cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         auto add = [&](int op, int lc, long long l0, long long l1, long long r0, long long r1, long long n) {
-            const int k = L->nblocks[op];
-            if (k >= MAX_SPLITS) {
+            if (cnt[op] >= MAX_SPLITS || nb >= MAX_RANGES) {
                 overfull = true;
                 return;
             }
-            BlockDesc &b = L->blocks[op][k];
+            if (cnt[op] == 0) s_first[op] = nb;
+            BlockDesc &b = s_blk[nb];
             b.op = op;
             b.lcost = lc;
             b.opmask = op == OP_NEG ? 1 : op == OP_X ? 2 : op == OP_F ? 4 : op == OP_G ? 8 : 0;
@@ -115,7 +134,7 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
             b.r0 = r0;
             b.r1 = r1;
             b.candidates = n;
-            L->nblocks[op] = k + 1;
+            ++cnt[op];
             cands += (u64)n;
         };
         auto unary = [&](int op, int k) {
@@ -149,33 +168,31 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
         const int ur = small ? A.nwarps * UNARY_ROWS : A.unary_rows_big;
         L->right_chunk = rc;
         L->unary_rows = ur;
-        L->check_only = L->on_the_fly;
+        L->check_only = on_the_fly;
         L->level_cands = cands;
         if (c < MAX_COSTS + 1) A.level_cands[c] = cands;
-        const bool fuse = !(L->plan_flags & PLAN_UNFUSED);
+        const bool fuse = !(flags & PLAN_UNFUSED);
         // Unary blocks: one per operator, or (fused) one per distinct source range with every
         // operator on it.
         int nu = 0;
         for (int j = 0; j < 4; ++j) {
             const int op = unary_slot_op(j);
-            if (L->nblocks[op] == 0) continue;
-            const BlockDesc &b = L->blocks[op][0];
+            if (cnt[op] == 0) continue;
+            const BlockDesc &b = s_blk[s_first[op]];
             int u = 0;
-            while (fuse && u < nu && !(L->ublocks[u].r0 == b.r0 && L->ublocks[u].r1 == b.r1)) ++u;
+            while (fuse && u < nu && !(s_ub[u].r0 == b.r0 && s_ub[u].r1 == b.r1)) ++u;
             if (!fuse || u == nu) {
                 u = nu++;
-                BlockDesc &f = L->ublocks[u];
-                f = b;
-                f.opmask = 0;
-                f.candidates = 0;
+                s_ub[u] = b;
+                s_ub[u].opmask = 0;
+                s_ub[u].candidates = 0;
             }
-            L->ublocks[u].opmask |= 1 << j;
-            L->ublocks[u].candidates += b.candidates;
+            s_ub[u].opmask |= 1 << j;
+            s_ub[u].candidates += b.candidates;
         }
-        L->nublocks = nu;
         int ne = 0;
         for (int u = 0; u < nu; ++u) {
-            BlockDesc &f = L->ublocks[u];
+            BlockDesc &f = s_ub[u];
             f.items = (f.r1 - f.r0 + ur - 1) / ur;
             f.tiles_r = 1;
             s_ent[ne] = ItemRange{f.items, 0, 1, u};
@@ -185,8 +202,8 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
             long long items = 0;
             const bool bin = op == OP_AND || op == OP_OR || op == OP_U;
             const int tile = op == OP_U ? A.left_tile / 2 : A.left_tile;
-            for (int k = 0; k < L->nblocks[op]; ++k) {
-                BlockDesc &b = L->blocks[op][k];
+            for (int k = 0; k < cnt[op]; ++k) {
+                BlockDesc &b = s_blk[s_first[op] + k];
                 b.item0 = items;
                 if (bin) {
                     b.tiles_r = (b.r1 - b.r0 + rc - 1) / rc;
@@ -199,17 +216,32 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
                 }
                 items += b.items;
             }
+            L->nblocks[op] = cnt[op];
             L->total_items[op] = items;
             L->item_hi[op] = items;
         }
+        L->nblocks[7] = 0;
+        L->nublocks = nu;
+        s_nblk = nb;
+        s_nu = nu;
         s_nent = ne;  // item0 holds each entry's item count until the table is laid out
         long long items = 0;
         for (int e = 0; e < ne; ++e) items += s_ent[e].item0;
         // order only matters when the level's items do not all start in the first wave
-        s_go = (L->plan_flags & PLAN_LEARNED) && A.model && items > A.grid ? 2 : 1;
+        s_go = (flags & PLAN_LEARNED) && A.model && items > A.grid ? 2 : 1;
     } while (0);
     __syncthreads();
     if (s_go == 0) return;
+    {  // the plan's blocks and unary blocks into global memory, all threads
+        const int nb = s_nblk, nu = s_nu;
+        constexpr int W = sizeof(BlockDesc) / 8;
+        for (int i = threadIdx.x; i < (nb + nu) * W; i += blockDim.x) {
+            const int e = i / W, w = i % W;
+            const BlockDesc &src = e < nb ? s_blk[e] : s_ub[e - nb];
+            BlockDesc &dst = e < nb ? L->blocks[src.op][src.pad - s_first[src.op]] : L->ublocks[e - nb];
+            reinterpret_cast<u64 *>(&dst)[w] = reinterpret_cast<const u64 *>(&src)[w];
+        }
+    }
     const int ne = s_nent;
     if (s_go == 2) {
         // Score every block (one warp per block).  A fused unary entry holds several
@@ -218,8 +250,7 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
         // go first and, of two equally likely ones, the smaller.
         const MlpDev &M = *reinterpret_cast<const MlpDev *>(A.model);
         const int c = L->cost;
-        const int nbl = L->nblocks[0] + L->nblocks[1] + L->nblocks[2] + L->nblocks[3] + L->nblocks[4] +
-                        L->nblocks[5] + L->nblocks[6];
+        const int nbl = s_nblk;
         const int jobs = ne * 4;  // (entry, unary slot); binary entries use slot 0 only
         for (int j = threadIdx.x; j < jobs; j += blockDim.x) s_q[j] = 1.0f;
         __syncthreads();
@@ -229,13 +260,13 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
             int op;
             const BlockDesc *b;
             if (R.cls == 1) {
-                if (!((L->ublocks[R.idx].opmask >> slot) & 1)) continue;
+                if (!((s_ub[R.idx].opmask >> slot) & 1)) continue;
                 op = unary_slot_op(slot);
-                b = &L->blocks[op][0];
+                b = &s_blk[s_first[op]];
             } else {
                 if (slot) continue;
                 op = R.idx / MAX_SPLITS;
-                b = &L->blocks[op][R.idx % MAX_SPLITS];
+                b = &s_blk[s_first[op] + R.idx % MAX_SPLITS];
             }
             if (lane == 0) {
                 const BlockInfo bi = block_info(*b, op, c, A.cf, nbl, (long long)L->level_cands, A.lstats, A.npos,
@@ -252,8 +283,9 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
             s_score[t] = s_q[4 * t] * s_q[4 * t + 1] * s_q[4 * t + 2] * s_q[4 * t + 3];
         __syncthreads();
         for (int t = threadIdx.x; t < ne; t += blockDim.x) {
-            const long long cands = s_ent[t].cls == 1 ? L->ublocks[s_ent[t].idx].candidates
-                                                       : L->blocks[s_ent[t].idx / MAX_SPLITS][s_ent[t].idx % MAX_SPLITS].candidates;
+            const int idx = s_ent[t].idx;
+            const long long cands = s_ent[t].cls == 1 ? s_ub[idx].candidates
+                                                       : s_blk[s_first[idx / MAX_SPLITS] + idx % MAX_SPLITS].candidates;
             s_score[t] = (1.0f - s_score[t]) / sqrtf((float)(cands > 0 ? cands : 1));
         }
         __syncthreads();

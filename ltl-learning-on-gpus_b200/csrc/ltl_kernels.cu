@@ -847,15 +847,19 @@ __global__ void __launch_bounds__(256, 3) level_kernel(const LevelArgs *__restri
 template <int HK>
 __global__ void insert_letters_kernel(const LevelArgs *__restrict__ pA, int nalpha) {
     const LevelArgs &A = *pA;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, j = threadIdx.x >> 5;  // warp j: letter j
     const int nch = A.pitch >> 1;
     const ulonglong2 *meta = reinterpret_cast<const ulonglong2 *>(A.wmeta);
-    for (int j = 0; j < nalpha; ++j) {
-        const u64 *row = A.cache + (u64)j * A.pitch;
+    const bool mine = j < nalpha;
+    const u64 *row = A.cache + (u64)(mine ? j : 0) * A.pitch;
+    const RowGen g{reinterpret_cast<const ulonglong2 *>(row)};
+    u64 fp = 0, kh = 0, kl = 0;
+    if (mine) {  // the letters' fingerprints and statistics, all letters at once
         u64 h[1] = {0};
-        u64 k = (2ull * lane + 1ull) * WEYL;
         u32 pm = 0, nh = 0;  // position 0: fails on a positive / holds on a negative
-        for (int c = lane; c < nch; c += 32, k += 64ull * WEYL) {
+#pragma unroll 4
+        for (int c = lane; c < nch; c += 32) {
+            const u64 k = (2ull * (u64)c + 1ull) * WEYL;
             const ulonglong2 w = reinterpret_cast<const ulonglong2 *>(row)[c];
             h[0] += hw<HK>(w.x, k, 2 * c < A.n) + hw<HK>(w.y, k + WEYL, 2 * c + 1 < A.n);
             const ulonglong2 m = meta[c];
@@ -866,65 +870,71 @@ __global__ void insert_letters_kernel(const LevelArgs *__restrict__ pA, int nalp
             count_row_stats(A.lstats + (u64)A.cf[0] * LSTATS, lane == 0, __any_sync(FULL, pm) ? 1u : 0u,
                             __any_sync(FULL, nh) ? 1u : 0u, lane);
         const u64 sum = reduce_to_lane<1>(h, lane);
-        u64 fp = fmix64(sum), kh = 0, kl = 0;
-        const RowGen g{reinterpret_cast<const ulonglong2 *>(row)};
+        fp = fmix64(sum);
         if (A.key_mode == KEY_HASH64) {
             kh = fp;
         } else if (A.key_mode == KEY_REF) {
             ref_key(A, g, 0, lane, kh, kl);
             fp = fmix64(kh ^ fmix64(kl + 0x5ad0dedull));
         }
-        // Probe with lane 0; a fingerprint match is verified by the whole warp.
-        const u64 tagbits = (fp >> 40) << 40, genbits = (u64)A.gen << 32;
-        u64 idx = fp & A.slot_mask;
-        for (u64 probe = 0; probe <= A.slot_mask; ++probe, idx = (idx + 1) & A.slot_mask) {
-            u64 v = 0;
-            int action = 0;  // 0 next, 1 claimed, 2 compare
-            if (lane == 0) {
-                v = ld_acquire(A.slots + idx);
-                if (slot_free(v, A.gen)) {
-                    const u64 old = atomicCAS(A.slots + idx, v, tagbits | genbits | (u64)(j + 1));
-                    if (old == v) {
-                        action = 1;
-                    } else {
-                        v = old;
-                    }
-                }
-                if (action == 0 && (v >> 40) == (tagbits >> 40) && (u32)v < FIELD_OVERFLOW) action = 2;
-            }
-            action = __shfl_sync(FULL, action, 0);
-            v = __shfl_sync(FULL, v, 0);
-            if (action == 1) {
+    }
+    // Registration in letter order, one warp at a time (a duplicate letter stays a row but
+    // the set keeps the first one, as the reference's sequential inserts do).
+    for (int turn = 0; turn < nalpha; ++turn) {
+        if (turn == j) {
+            // Probe with lane 0; a fingerprint match is verified by the whole warp.
+            const u64 tagbits = (fp >> 40) << 40, genbits = (u64)A.gen << 32;
+            u64 idx = fp & A.slot_mask;
+            for (u64 probe = 0; probe <= A.slot_mask; ++probe, idx = (idx + 1) & A.slot_mask) {
+                u64 v = 0;
+                int action = 0;  // 0 next, 1 claimed, 2 compare
                 if (lane == 0) {
-                    A.parents[j] = pack_parent(OP_ATOM, 0, 0);
-                    if (A.keys) {
-                        A.keys[2 * j] = kh;
-                        A.keys[2 * j + 1] = kl;
+                    v = ld_acquire(A.slots + idx);
+                    if (slot_free(v, A.gen)) {
+                        const u64 old = atomicCAS(A.slots + idx, v, tagbits | genbits | (u64)(j + 1));
+                        if (old == v) {
+                            action = 1;
+                        } else {
+                            v = old;
+                        }
                     }
+                    if (action == 0 && (v >> 40) == (tagbits >> 40) && (u32)v < FIELD_OVERFLOW) action = 2;
                 }
-                break;
-            }
-            if (action == 2) {
-                const u64 other = (u64)(u32)v - 1;
-                bool same;
-                if (A.key_mode == KEY_EXACT) {
-                    bool diff = false;
-                    const ulonglong2 *ex = reinterpret_cast<const ulonglong2 *>(A.cache + other * A.pitch);
-                    for (int c = lane; c < nch; c += 32) {
-                        const ulonglong2 a = g.word(0, c, g.pre(c)), b = __ldcg(ex + c);
-                        diff |= (a.x != b.x) | (a.y != b.y);
+                action = __shfl_sync(FULL, action, 0);
+                v = __shfl_sync(FULL, v, 0);
+                if (action == 1) {
+                    if (lane == 0) {
+                        A.parents[j] = pack_parent(OP_ATOM, 0, 0);
+                        if (A.keys) {
+                            A.keys[2 * j] = kh;
+                            A.keys[2 * j + 1] = kl;
+                        }
                     }
-                    same = !__any_sync(FULL, diff);
-                } else {
-                    same = A.keys[2 * other] == kh && A.keys[2 * other + 1] == kl;
-                }
-                if (same) {
-                    if (lane == 0) A.parents[j] = pack_parent(OP_ATOM, 0, 0);
                     break;
                 }
+                if (action == 2) {
+                    const u64 other = (u64)(u32)v - 1;
+                    bool same;
+                    if (A.key_mode == KEY_EXACT) {
+                        bool diff = false;
+                        const ulonglong2 *ex = reinterpret_cast<const ulonglong2 *>(A.cache + other * A.pitch);
+                        for (int c = lane; c < nch; c += 32) {
+                            const ulonglong2 a = g.word(0, c, g.pre(c)), b = __ldcg(ex + c);
+                            diff |= (a.x != b.x) | (a.y != b.y);
+                        }
+                        same = !__any_sync(FULL, diff);
+                    } else {
+                        same = A.keys[2 * other] == kh && A.keys[2 * other + 1] == kl;
+                    }
+                    if (same) {
+                        if (lane == 0) A.parents[j] = pack_parent(OP_ATOM, 0, 0);
+                        break;
+                    }
+                }
             }
+            __threadfence();
         }
-        __syncwarp();
+        __syncthreads();
     }
 }
 
@@ -1083,9 +1093,9 @@ int level_kernel_max_ctas_per_sm(int left_tile, int hash_kind, int block, int pi
 
 cudaError_t launch_insert_letters(const LevelArgs &a, const LevelArgs *d, int nalpha, cudaStream_t s) {
     if (a.hash_kind == 1)
-        insert_letters_kernel<1><<<1, 32, 0, s>>>(d, nalpha);
+        insert_letters_kernel<1><<<1, 32 * (nalpha > 0 ? nalpha : 1), 0, s>>>(d, nalpha);
     else
-        insert_letters_kernel<0><<<1, 32, 0, s>>>(d, nalpha);
+        insert_letters_kernel<0><<<1, 32 * (nalpha > 0 ? nalpha : 1), 0, s>>>(d, nalpha);
     return cudaGetLastError();
 }
 

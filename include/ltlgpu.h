@@ -86,7 +86,8 @@ typedef struct ltlg_engine_config {
     int32_t left_tile;         /* left rows staged in shared memory per binary work item: 4, 8 or 16 */
     int32_t right_chunk;       /* right rows per binary work item */
     int32_t unary_rows;        /* source rows per unary work item */
-    int32_t pad_;
+    int32_t small_rows;        /* levels below the small-level size: right rows (unary: source-row
+                                  pairs) per warp and work item; 0 = 1 */
 } ltlg_engine_config;
 
 typedef struct ltlg_options {

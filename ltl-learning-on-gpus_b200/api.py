@@ -46,7 +46,7 @@ class EngineConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("slots_log2", C.c_int32), ("cache_bytes", C.c_int64),
                 ("max_rows", C.c_int64), ("max_traces", C.c_int32), ("block_threads", C.c_int32),
                 ("left_tile", C.c_int32), ("right_chunk", C.c_int32), ("unary_rows", C.c_int32),
-                ("pad_", C.c_int32)]
+                ("small_rows", C.c_int32)]
 
 
 class Options(C.Structure):
@@ -218,13 +218,13 @@ class Engine:
     """Device state for repeated learns: language cache, hash set, stream."""
 
     def __init__(self, device=0, slots_log2=27, cache_bytes=16 << 30, max_rows=64 << 20, max_traces=8192,
-                 block_threads=256, left_tile=8, right_chunk=64, unary_rows=64):
+                 block_threads=256, left_tile=8, right_chunk=16, unary_rows=32, small_rows=1):
         L = lib()
         cfg = EngineConfig()
         L.ltlg_default_engine_config(C.byref(cfg))
         cfg.device, cfg.slots_log2, cfg.cache_bytes, cfg.max_rows = device, slots_log2, cache_bytes, max_rows
         cfg.max_traces, cfg.block_threads, cfg.left_tile = max_traces, block_threads, left_tile
-        cfg.right_chunk, cfg.unary_rows = right_chunk, unary_rows
+        cfg.right_chunk, cfg.unary_rows, cfg.small_rows = right_chunk, unary_rows, small_rows
         h = C.c_void_p()
         rc = L.ltlg_engine_create(C.byref(cfg), C.byref(h))
         if rc != 0:
@@ -316,12 +316,12 @@ class Engine:
 
 
 def _engine_config(device=0, slots_log2=27, cache_bytes=16 << 30, max_rows=64 << 20, max_traces=8192,
-                   block_threads=256, left_tile=8, right_chunk=64, unary_rows=64) -> EngineConfig:
+                   block_threads=256, left_tile=8, right_chunk=16, unary_rows=32, small_rows=1) -> EngineConfig:
     cfg = EngineConfig()
     lib().ltlg_default_engine_config(C.byref(cfg))
     cfg.device, cfg.slots_log2, cfg.cache_bytes, cfg.max_rows = device, slots_log2, cache_bytes, max_rows
     cfg.max_traces, cfg.block_threads, cfg.left_tile = max_traces, block_threads, left_tile
-    cfg.right_chunk, cfg.unary_rows = right_chunk, unary_rows
+    cfg.right_chunk, cfg.unary_rows, cfg.small_rows = right_chunk, unary_rows, small_rows
     return cfg
 
 

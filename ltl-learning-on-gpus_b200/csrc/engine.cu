@@ -222,8 +222,9 @@ LTLG_API void ltlg_default_engine_config(ltlg_engine_config *c) {
     c->max_traces = 8192;
     c->block_threads = 256;
     c->left_tile = 8;
-    c->right_chunk = 64;
-    c->unary_rows = 64;
+    c->right_chunk = 16;
+    c->unary_rows = 32;
+    c->small_rows = 1;
 }
 
 LTLG_API void ltlg_default_options(ltlg_options *o) {
@@ -525,6 +526,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     A.right_chunk_big = e->cfg.right_chunk;
     A.unary_rows_big = e->cfg.unary_rows;
     A.small_level = max_grid * 2048ll;
+    A.small_rows = std::max(1, e->cfg.small_rows);
     A.hash_kind = hk;
     A.cap_rows = cap_rows;
     A.cache = (u64 *)e->cache.p;

@@ -124,6 +124,7 @@ struct LevelArgs {
     int nwarps;
     int cf[8];           // costs of p ~ & | X F G U
     int right_chunk_big, unary_rows_big;
+    int small_rows;      // small levels: right rows (unary: source-row pairs) per warp and item
     int hash_kind;       // fingerprint kind of the operator kernels (0 multiply-add, 1 fmix64)
     long long small_level;  // levels with fewer candidates use one row per warp per item
     long long cap_rows;

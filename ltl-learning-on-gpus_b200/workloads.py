@@ -135,7 +135,7 @@ def cfg4_specs(count: int = 4096, seed: int = 0):
 
 
 AUTOTUNE_SPACE = [dict(left_tile=lt, right_chunk=rc, unary_rows=ur, slots_log2=sl, workers=w)
-                  for lt in (4, 8) for rc in (32, 64) for ur in (32, 64) for sl in (20, 22) for w in (8, 16)]
+                  for lt in (4, 8) for rc in (16, 64) for ur in (32, 64) for sl in (20, 22) for w in (8, 16)]
 
 
 def autotune(sample, space=AUTOTUNE_SPACE, cache_bytes=1 << 30, repeats=2, device=0, **opts):

@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--small-rows", type=int, default=1, help="small levels: right rows per warp and item")
     ap.add_argument("--right-chunk", type=int, default=16, help="large levels: right rows per binary item")
     ap.add_argument("--unary-rows", type=int, default=32, help="large levels: source rows per unary item")
+    ap.add_argument("--left-tile", type=int, default=4, help="left rows staged in shared memory per binary item")
+    ap.add_argument("--block-threads", type=int, default=256)
     ap.add_argument("--cpu-sample-s", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
@@ -295,7 +297,8 @@ def run_ours(a):
     from ltlb200 import api
     batch = make_batch(seeds_of(a.seeds, rank))
     ekw = dict(device=local, slots_log2=a.slots_log2, cache_bytes=int(a.cache_gb * (1 << 30)), small_rows=a.small_rows,
-               right_chunk=a.right_chunk, unary_rows=a.unary_rows)
+               right_chunk=a.right_chunk, unary_rows=a.unary_rows, left_tile=a.left_tile,
+               block_threads=a.block_threads)
     eng = api.Engine(**ekw)
     pool = api.Batch(workers=a.workers, **ekw) if a.workers > 0 else None
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")

@@ -218,7 +218,7 @@ class Engine:
     """Device state for repeated learns: language cache, hash set, stream."""
 
     def __init__(self, device=0, slots_log2=27, cache_bytes=16 << 30, max_rows=64 << 20, max_traces=8192,
-                 block_threads=256, left_tile=8, right_chunk=16, unary_rows=32, small_rows=1):
+                 block_threads=256, left_tile=4, right_chunk=16, unary_rows=32, small_rows=1):
         L = lib()
         cfg = EngineConfig()
         L.ltlg_default_engine_config(C.byref(cfg))
@@ -316,7 +316,7 @@ class Engine:
 
 
 def _engine_config(device=0, slots_log2=27, cache_bytes=16 << 30, max_rows=64 << 20, max_traces=8192,
-                   block_threads=256, left_tile=8, right_chunk=16, unary_rows=32, small_rows=1) -> EngineConfig:
+                   block_threads=256, left_tile=4, right_chunk=16, unary_rows=32, small_rows=1) -> EngineConfig:
     cfg = EngineConfig()
     lib().ltlg_default_engine_config(C.byref(cfg))
     cfg.device, cfg.slots_log2, cfg.cache_bytes, cfg.max_rows = device, slots_log2, cache_bytes, max_rows

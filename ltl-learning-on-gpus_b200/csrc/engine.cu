@@ -221,7 +221,7 @@ LTLG_API void ltlg_default_engine_config(ltlg_engine_config *c) {
     c->max_rows = 64ll << 20;
     c->max_traces = 8192;
     c->block_threads = 256;
-    c->left_tile = 8;
+    c->left_tile = 4;
     c->right_chunk = 16;
     c->unary_rows = 32;
     c->small_rows = 1;

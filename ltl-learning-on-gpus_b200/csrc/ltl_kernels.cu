@@ -749,8 +749,10 @@ __device__ __forceinline__ int find_block(const BlockDesc *blocks, int nb, long 
 // number.  A unary item is A.unary_rows source rows of a unary block (every operator of its
 // mask on each row); a binary item stages a tile of left rows in shared memory with one bulk
 // copy, and the CTA's warps take the item's right rows one at a time.
+// Three CTAs per SM with an 8-row tile (64 KB of shared memory at n = 1000); four with a
+// 4-row tile, which caps registers at 64 (measured faster end to end than 80 at three).
 template <int TL, int HK>
-__global__ void __launch_bounds__(256, 3) level_kernel(const LevelArgs *__restrict__ A0) {
+__global__ void __launch_bounds__(256, TL == 4 ? 4 : 3) level_kernel(const LevelArgs *__restrict__ A0) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     u64 *tile = reinterpret_cast<u64 *>(smem_raw);
     __shared__ __align__(16) LevelArgs A;

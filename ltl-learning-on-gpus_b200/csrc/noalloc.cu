@@ -260,6 +260,7 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     for (int i = 0; i < 8; ++i) A.cf[i] = cf[i];
     A.right_chunk_big = 64;
     A.unary_rows_big = 64;
+    A.small_rows = 1;
     A.small_level = max_grid * 2048ll;
     A.hash_kind = hk;
     A.cap_rows = cap;

@@ -164,8 +164,9 @@ __global__ void __launch_bounds__(256) plan_kernel(const LevelArgs *__restrict__
         // Work-item size: a small level is cut into one right row (or one group of source
         // rows) per warp so every SM takes part; a large level keeps the configured sizes.
         const bool small = (long long)cands < A.small_level;
-        const int rc = small ? A.nwarps * A.small_rows : A.right_chunk_big;
-        const int ur = small ? A.nwarps * UNARY_ROWS * A.small_rows : A.unary_rows_big;
+        const int sr = A.small_rows > 1 ? A.small_rows : 1;
+        const int rc = max(1, small ? A.nwarps * sr : A.right_chunk_big);
+        const int ur = max(1, small ? A.nwarps * UNARY_ROWS * sr : A.unary_rows_big);
         L->right_chunk = rc;
         L->unary_rows = ur;
         L->check_only = on_the_fly;

@@ -83,7 +83,7 @@ typedef struct ltlg_engine_config {
     int64_t max_rows;          /* upper bound on cache rows (<= 2^30); 0 = budget only */
     int32_t max_traces;        /* largest n the engine accepts */
     int32_t block_threads;     /* threads per CTA of the level kernel (multiple of 32) */
-    int32_t left_tile;         /* left rows staged in shared memory per binary work item: 4, 8 or 16 */
+    int32_t left_tile;         /* left rows staged in shared memory per binary work item: 2, 4 or 8 */
     int32_t right_chunk;       /* right rows per binary work item */
     int32_t unary_rows;        /* source rows per unary work item */
     int32_t small_rows;        /* levels below the small-level size: right rows (unary: source-row

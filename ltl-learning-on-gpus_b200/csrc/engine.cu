@@ -250,7 +250,7 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
         ltlg_default_engine_config(&cfg);
     if (cfg.device < 0 || cfg.device >= ndev) return LTLG_BAD_ARGS;
     if (cfg.slots_log2 < 10 || cfg.slots_log2 > 34) return LTLG_BAD_ARGS;
-    if (cfg.left_tile != 4 && cfg.left_tile != 8) return LTLG_BAD_ARGS;
+    if (cfg.left_tile != 2 && cfg.left_tile != 4 && cfg.left_tile != 8) return LTLG_BAD_ARGS;
     if (cfg.block_threads < 32 || cfg.block_threads > 256 || cfg.block_threads % 32) return LTLG_BAD_ARGS;
     if (cfg.right_chunk < 1 || cfg.unary_rows < 1 || cfg.max_traces < 1) return LTLG_BAD_ARGS;
     if (cfg.max_rows <= 0 || cfg.max_rows > (1ll << 30) - 1) cfg.max_rows = (1ll << 30) - 1;
@@ -493,7 +493,8 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     cudaMemcpyAsync(e->ctl.p, hc, sizeof(DevCtl), cudaMemcpyHostToDevice, st);
 
     int tl = e->cfg.left_tile;
-    while (tl > 4 && (size_t)level_kernel_smem_bytes(tl, pitch) > 200 * 1024) tl /= 2;
+    // shrink the left tile until three CTAs fit an SM's shared memory (long CS rows)
+    while (tl > 2 && 3 * (size_t)level_kernel_smem_bytes(tl, pitch) > 200 * 1024) tl /= 2;
     if ((size_t)level_kernel_smem_bytes(tl, pitch) > 220 * 1024) {
         res->status = LTLG_BAD_ARGS;
         res->formula = strdup("bad_arguments");

@@ -750,9 +750,9 @@ __device__ __forceinline__ int find_block(const BlockDesc *blocks, int nb, long 
 // mask on each row); a binary item stages a tile of left rows in shared memory with one bulk
 // copy, and the CTA's warps take the item's right rows one at a time.
 // Three CTAs per SM with an 8-row tile (64 KB of shared memory at n = 1000); four with a
-// 4-row tile, which caps registers at 64 (measured faster end to end than 80 at three).
+// 4- or 2-row tile, which caps registers at 64 (measured faster end to end than 80 at three).
 template <int TL, int HK>
-__global__ void __launch_bounds__(256, TL == 4 ? 4 : 3) level_kernel(const LevelArgs *__restrict__ A0) {
+__global__ void __launch_bounds__(256, TL <= 4 ? 4 : 3) level_kernel(const LevelArgs *__restrict__ A0) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     u64 *tile = reinterpret_cast<u64 *>(smem_raw);
     __shared__ __align__(16) LevelArgs A;
@@ -1084,13 +1084,22 @@ static int occupancy_tl(int block, int pitch) {
 
 cudaError_t launch_level(const LevelArgs &a, const LevelArgs *d, int grid, int block, cudaStream_t s) {
     if (a.hash_kind == 1)
-        return a.left_tile == 4 ? launch_tl<4, 1>(a, d, grid, block, s) : launch_tl<8, 1>(a, d, grid, block, s);
-    return a.left_tile == 4 ? launch_tl<4, 0>(a, d, grid, block, s) : launch_tl<8, 0>(a, d, grid, block, s);
+        return a.left_tile == 2   ? launch_tl<2, 1>(a, d, grid, block, s)
+               : a.left_tile == 4 ? launch_tl<4, 1>(a, d, grid, block, s)
+                                  : launch_tl<8, 1>(a, d, grid, block, s);
+    return a.left_tile == 2   ? launch_tl<2, 0>(a, d, grid, block, s)
+           : a.left_tile == 4 ? launch_tl<4, 0>(a, d, grid, block, s)
+                              : launch_tl<8, 0>(a, d, grid, block, s);
 }
 
 int level_kernel_max_ctas_per_sm(int left_tile, int hash_kind, int block, int pitch) {
-    if (hash_kind == 1) return left_tile == 4 ? occupancy_tl<4, 1>(block, pitch) : occupancy_tl<8, 1>(block, pitch);
-    return left_tile == 4 ? occupancy_tl<4, 0>(block, pitch) : occupancy_tl<8, 0>(block, pitch);
+    if (hash_kind == 1)
+        return left_tile == 2   ? occupancy_tl<2, 1>(block, pitch)
+               : left_tile == 4 ? occupancy_tl<4, 1>(block, pitch)
+                                : occupancy_tl<8, 1>(block, pitch);
+    return left_tile == 2   ? occupancy_tl<2, 0>(block, pitch)
+           : left_tile == 4 ? occupancy_tl<4, 0>(block, pitch)
+                            : occupancy_tl<8, 0>(block, pitch);
 }
 
 cudaError_t launch_insert_letters(const LevelArgs &a, const LevelArgs *d, int nalpha, cudaStream_t s) {

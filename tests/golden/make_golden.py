@@ -10,9 +10,9 @@ so they are made here:
   2. ``make -C oracle ref``  (in a checkout that has the reference sources)
         compiles code/ltli6463.cu twice into oracle/_ref/: with and without
         -D MEASUREMENT_MODE;
-  3. ``python tests/golden/make_golden.py run --out gpurun_out/golden_raw``  (on a B200)
+  3. ``python tests/golden/make_golden.py run --out <raw dir>``  (on a B200)
         runs both binaries on every manifest entry and keeps their stdout;
-  4. ``python tests/golden/make_golden.py collect --raw gpurun_out/golden_raw``
+  4. ``python tests/golden/make_golden.py collect --raw <raw dir>``
         parses the outputs into tests/golden/reference_runs.json.
 
 Only step 3 needs a GPU; steps 1 and 4 and the tests that read the JSON do not.

@@ -571,9 +571,10 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     const u32 fatal = ST_WAIT | ST_TMA | ST_TABLE;
     auto fatal_status = [&](u32 f) { return (f & ST_TABLE) ? LTLG_TABLE_FULL : LTLG_DEVICE_WAIT; };
 
-    // ---- device-planned levels: per level a one-thread planner (plan from the level starts
-    // in device memory) and the level kernel, enqueued up to RING - 1 levels ahead of the
-    // level the host is reading, so the GPU never waits for the host between levels.
+    // ---- device-planned levels: per level one graph launch (the planner builds the plan from
+    // the level starts in device memory, then the level kernel runs it and its last CTA writes
+    // the level summary into the mapped host ring), enqueued up to RING - 1 levels ahead of
+    // the level the host is reading, so the GPU never waits for the host between levels.
     bool host_mode = per_block;
     std::vector<float> level_ms;
     if (!host_mode) {

@@ -4,11 +4,15 @@
 // from the level's (operator, split) blocks.  A binary item stages a tile of
 // left-operand CSs in shared memory with one bulk copy (cp.async.bulk, no
 // multicast) and streams right-operand CSs from HBM with 128-bit loads; every
-// warp evaluates a whole tile of candidates per right row in registers.  The
-// fused epilogue per candidate is: fingerprint (warp reduce-scatter),
-// acceptance (redux.sync over bit 0 of every word), and exact uniqueness in an
-// open-addressing HBM hash set (claim by CAS, write the row, publish; a
-// fingerprint match is verified word by word against the stored row).
+// warp evaluates a whole tile of candidates per right row in registers.  A unary
+// item applies every unary operator that reads the same source rows (~ X F G) to
+// one load of each source chunk.  The fused epilogue per candidate is:
+// fingerprint (warp reduce-scatter), acceptance (redux.sync over the positive-miss
+// and negative-hit masks of bit 0), exact uniqueness in an open-addressing HBM
+// hash set (claim by CAS, write the row, publish; a fingerprint match is verified
+// word by word against the stored row), and per-level row statistics for the
+// learned block order.  The last CTA of a launch writes the level's summary into
+// the host's mapped ring.
 //
 // Semantics follow MojtabaValizadeh/ltl-learning-on-gpus, code/ltli6463.cu:
 //   operators .......... :203-204 (~), :295 (&), :385 (|), :468 (X), :551-556 (F),

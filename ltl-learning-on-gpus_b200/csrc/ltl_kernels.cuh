@@ -59,7 +59,7 @@ struct BlockDesc {
 
 constexpr int MAX_SPLITS = 64;   // blocks per operator and level in a device-planned level
 constexpr int MAX_RANGES = 4 + 3 * MAX_SPLITS;  // entries of a level's item table
-constexpr int UNARY_ROWS = 2;    // source rows per unary work item (each with every operator of its mask)
+constexpr int UNARY_ROWS = 1;    // source rows per warp in a unary item (each with every operator of its mask)
 constexpr int MAX_COSTS = 512;   // level starts kept on the device
 constexpr int LSTATS = 2;        // row-statistics counters per cost (see count_row_stats)
 

@@ -101,3 +101,19 @@ def test_trained_scorer_gains_over_plain_order():
     s = learned.summarize(rows)
     assert s["same_cost"], rows
     assert sum(r["evaluated_learned"] for r in rows) < sum(r["evaluated_plain"] for r in rows), s
+
+
+def test_learned_order_with_per_block_schedule():
+    """Per-block launches under a learned order (windows of the sorted item table) find the
+    same minimal cost and the same level counts as the fused plain schedule."""
+    p = learned.init_params(11)
+    with api.Engine(slots_log2=22, cache_bytes=2 << 30) as eng:
+        eng.set_scorer(p)
+        for seed in range(3):
+            inst = learned.hamming_instance(seed + 20, 80, 80)
+            a = eng.learn(inst, neg_type=1, order=api.ORDER_LEARNED, schedule=api.SCHEDULE_PER_BLOCK,
+                          max_cost=6, stop_at_found=False, record_levels=True)
+            b = eng.learn(inst, neg_type=1, max_cost=6, stop_at_found=False, record_levels=True)
+            assert a.status == b.status and a.cost == b.cost
+            assert [(l["cost"], l["candidates"], l["uniques"]) for l in a.levels] == \
+                   [(l["cost"], l["candidates"], l["uniques"]) for l in b.levels]

@@ -144,7 +144,8 @@ typedef struct ltlg_result {
 
 typedef struct ltlg_engine ltlg_engine;
 
-/* Defaults: device 0, 2^27 slots, 16 GiB cache, n <= 8192, 256 threads, tiles 8/64/64. */
+/* Defaults: device 0, 2^27 slots, 16 GiB cache, n <= 8192, 256 threads, left tile 4,
+   right chunk 16, unary rows 32, small rows 1. */
 LTLG_API void ltlg_default_engine_config(ltlg_engine_config *cfg);
 /* The reference's defaults: unit costs, maxCost 500, type 3, NegType 2, exact keys, fused, plain. */
 LTLG_API void ltlg_default_options(ltlg_options *opt);

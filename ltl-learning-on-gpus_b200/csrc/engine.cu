@@ -1024,6 +1024,19 @@ LTLG_API int ltlg_learn(const ltlg_traces *t, const ltlg_options *opt, ltlg_resu
     ltlg_engine_config cfg;
     ltlg_default_engine_config(&cfg);
     const int n = t ? t->num_pos + t->num_neg : 0;
+    // The input limits are checked before the device is touched, as the reference checks
+    // them before its first device call (ltli6463.cu:1078-1083).
+    if (t && opt && res && t->offsets && t->num_pos >= 0 && t->num_neg >= 0) {
+        int max_len = 0;
+        for (int i = 0; i < n; ++i) max_len = std::max(max_len, t->offsets[i + 1] - t->offsets[i]);
+        if ((opt->limit_traces && n > 64) || max_len > 63) {
+            memset(res, 0, sizeof(*res));
+            res->status = LTLG_INPUT_LIMITS;
+            res->cost = opt->cost_fun[0];
+            res->formula = strdup(ltlg_status_string(LTLG_INPUT_LIMITS));
+            return res->status;
+        }
+    }
     const long long pitch = std::max(4, (n + 3) & ~3);
     // The reference sizes its cache from the pitch limit (ltli6463.cu:1152-1156): about
     // 3 GiB of rows.  Keep that budget, bounded by free memory.

@@ -183,6 +183,32 @@ class Driver:
         return f"({left})|({right})"
 
 
+def formula_size(ltl: str) -> int:
+    """The reference's formula size measure (code/dc.py:329-330, `c`): the characters of the
+    string other than ',', ' ', '(' and ')'."""
+    return sum(ch not in ",() " for ch in ltl)
+
+
+def over_fitted(alphabet, pos_lines) -> str:
+    """The reference's over-fitted formula for a set of positive traces (code/dc.py:332-356,
+    `LTLOfSingleTrace` and `overFittedCase`).  `alphabet` is the letters in the file's value
+    order; each line is a Scarlet trace ("1,0;0,1").  A trace becomes the chain
+    "l0&X(l1&X(... ln&~X(a|~a)))", li the conjunction of every letter or its negation at step
+    i and a the first letter (so the chain also says the trace ends there); several traces
+    are joined as "(f1)|(f2)|...".  The result is in the reference's infix form, not the
+    enumerator's fully parenthesised one."""
+    a0 = alphabet[0]
+    chains = []
+    for line in pos_lines:
+        steps = ["&".join(a if v == "1" else "~" + a for a, v in zip(alphabet, tok.split(",")))
+                 for tok in line.split(";")]
+        f = f"{steps[-1]}&~X({a0}|~{a0})"
+        for lit in reversed(steps[:-1]):
+            f = f"{lit}&X({f})"
+        chains.append(f)
+    return chains[0] if len(chains) == 1 else "|".join(f"({f})" for f in chains)
+
+
 def run_dc(base: Instance, algo: str = "rand", window: int = 64, timeout_s: float = 2000.0, engine=None,
            **opts) -> dict:
     """The reference's runDC (code/dc.py:368-387) on an instance: the formula (or 'Function

@@ -42,3 +42,71 @@ def test_window_covering_everything_is_one_call():
     f = d.det_split(64, list(range(12)), list(range(12)))
     assert d.calls == 1 and O.separates(f, inst)
     assert O.formula_cost(f) == O.learn(inst, neg_type=1, keep_rows=False).cost
+
+
+def test_formula_size_counts_symbols():
+    assert divide.formula_size("(p)&(q)") == 3
+    assert divide.formula_size("G(((p)&(q))|(~((p)|(q))))") == 9
+    assert divide.formula_size("p, q ") == 2
+
+
+def test_over_fitted_string():
+    assert divide.over_fitted("pq", ["1,0;0,1"]) == "p&~q&X(~p&q&~X(p|~p))"
+    assert divide.over_fitted("pq", ["1,1", "0,0"]) == "(p&q&~X(p|~p))|(~p&~q&~X(p|~p))"
+
+
+def _parenthesise(s):
+    """The reference's infix form (~ binds tightest, then &, then |) as the enumerator's fully
+    parenthesised form, so the oracle's evaluator can read it."""
+    pos = 0
+
+    def expr():
+        nonlocal pos
+        f = term()
+        while pos < len(s) and s[pos] == "|":
+            pos += 1
+            f = f"({f})|({term()})"
+        return f
+
+    def term():
+        nonlocal pos
+        f = factor()
+        while pos < len(s) and s[pos] == "&":
+            pos += 1
+            f = f"({f})&({factor()})"
+        return f
+
+    def factor():
+        nonlocal pos
+        c = s[pos]
+        if c == "~":
+            pos += 1
+            return f"~({factor()})"
+        if c in "XFG" and pos + 1 < len(s) and s[pos + 1] == "(":
+            pos += 2
+            f = expr()
+            assert s[pos] == ")"
+            pos += 1
+            return f"{c}({f})"
+        if c == "(":
+            pos += 1
+            f = expr()
+            assert s[pos] == ")"
+            pos += 1
+            return f
+        pos += 1
+        return c
+
+    out = expr()
+    assert pos == len(s)
+    return out
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_over_fitted_holds_exactly_on_the_positive_traces(seed):
+    inst = gen.generate(seed, 3, 12, 12, 2, 6, 0.5, 4)
+    lines = inst.trace_lines()
+    f = _parenthesise(divide.over_fitted(inst.alphabet, lines[:inst.num_pos]))
+    h = O.evaluate(f, inst)
+    expect = np.array([ln in set(lines[:inst.num_pos]) for ln in lines], dtype=bool)
+    assert np.array_equal(h.astype(bool), expect)

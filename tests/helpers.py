@@ -37,3 +37,23 @@ def row_set(rows: np.ndarray) -> set:
 
 def lensum(inst):
     return int(np.asarray(inst.lengths).sum())
+
+
+def last_round_gap(costs):
+    """Levels the reference runs on the fly after the one that overflowed: the first cost
+    difference that matches an operator's reach (ltli6463.cu:1202-1206)."""
+    c1, c2, c3, c4, c5, c6, c7, c8 = costs
+    return min(c2, c1 + c3, c1 + c4, c5, c6, c7, c1 + c8)
+
+
+def on_the_fly_cases(inst, costs, max_cost=14):
+    """(k, cache rows) for caches that hold exactly the rows through level k while level k + 1
+    has new CSs: the overflow then stores nothing of level k + 1, so the regime that follows
+    is deterministic.  The cache holds at least one row beyond the letters."""
+    import oracle as O
+
+    ex = O.learn(inst, costs=costs, neg_type=1, max_cost=max_cost)
+    assert ex.status == O.FOUND
+    return ex, [(k, ex.level_start[k + 1]) for k in range(costs[0] + 1, ex.cost - 1)
+                if ex.level_start[k + 2] > ex.level_start[k + 1] > len(inst.alphabet)]
+

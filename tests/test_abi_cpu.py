@@ -79,3 +79,12 @@ def test_hamming_negatives_are_near_misses():
         assert best is not None and 1 <= best <= 3
     cs = h.atom_cs()
     assert cs.shape[0] == 4
+
+
+def test_one_shot_learn_checks_limits_before_the_device():
+    """ltlg_learn refuses traces longer than 63 steps before it looks for a device, as the
+    reference checks its limits before its first device call (ltli6463.cu:1078-1083)."""
+    res = api.learn(load_fixture("len64.trace"), costs=(2, 1, 1, 1, 1, 1, 1, 1))
+    assert res.status == api.INPUT_LIMITS and res.formula == "see_the_error" and res.cost == 2
+    over = load_fixture("over64.trace")
+    assert api.learn(over, limit_traces=True).status == api.INPUT_LIMITS

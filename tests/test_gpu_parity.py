@@ -7,7 +7,7 @@ import pytest
 
 import oracle as O
 from ltlb200 import api, gen
-from helpers import load_fixture, lensum, row_set
+from helpers import last_round_gap, lensum, load_fixture, on_the_fly_cases, row_set
 
 pytestmark = pytest.mark.gpu
 
@@ -161,6 +161,29 @@ def test_letter_hit_and_limits(engine):
     ref = O.learn(over)
     assert res.cost == ref.cost
 
+
+
+@pytest.mark.parametrize("costs", [(1,) * 8, (1, 2, 1, 1, 2, 2, 2, 2)])
+def test_on_the_fly_regime_matches_oracle(costs):
+    """Caches that hold exactly the rows through level k: level k + 1 overflows, the engine
+    switches to the reference's on-the-fly regime (ltli6463.cu:1021-1027, 1202-1206,
+    1442-1443) and checks the following levels without storing; status, cost, candidate
+    count and the switch equal the oracle's, and a find separates the traces."""
+    inst = gen.generate(3, 3, 30, 30, 6, 14, 0.5, 7)
+    ex, cases = on_the_fly_cases(inst, costs)
+    assert len(cases) >= 3
+    for k, cap in cases:
+        ref = O.learn(inst, costs=costs, neg_type=1, max_cost=14, cache_rows=cap, keep_rows=False)
+        with api.Engine(slots_log2=20, cache_bytes=64 << 20, max_rows=cap) as e:
+            res = e.learn(inst, costs=costs, neg_type=1, max_cost=14)
+        assert res.device_flags & ~1 == 0, (k, res.device_flags)
+        assert res.on_the_fly and ref.on_the_fly and res.rows == cap, k
+        assert (res.status, res.cost) == ((api.FOUND if ref.status == O.FOUND else api.NOT_FOUND), ref.cost), k
+        if res.status == api.FOUND:
+            assert O.separates(res.formula, inst) and O.formula_cost(res.formula, costs) == res.cost
+        else:
+            assert res.cost == k + 1 + last_round_gap(costs)
+            assert res.all_ltls == ref.all_ltls, k
 
 def test_engine_reuse_many_instances(engine):
     # hash-set generations: later instances must not see earlier instances' slots

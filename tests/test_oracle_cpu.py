@@ -9,7 +9,7 @@ import pytest
 
 import oracle as O
 from ltlb200 import gen
-from helpers import load_fixture, row_set
+from helpers import last_round_gap, load_fixture, on_the_fly_cases, row_set
 
 OPS = ["~", "&", "|", "X", "F", "G", "U"]
 
@@ -197,3 +197,27 @@ def test_relaxed_type3_collides_where_exact_does_not():
     assert rlx.num_rows <= exact.num_rows
     h64 = O.learn(inst, max_cost=6, stop_at_found=False, key_mode=O.KEY_HASH64)
     assert h64.num_rows == exact.num_rows  # no 64-bit fingerprint collision at this size
+
+
+OTF_COSTS = [(1,) * 8, (1, 2, 1, 1, 2, 2, 2, 2)]
+
+@pytest.mark.parametrize("costs", OTF_COSTS)
+def test_oracle_on_the_fly_regime(costs):
+    """The reference's overflow switch (ltli6463.cu:1021-1027, 1202-1206, 1442-1443): once a
+    level finds no free cache row, later levels are only checked for acceptance, built from
+    the stored rows, until the last-round rule ends the search."""
+    inst = gen.generate(3, 3, 30, 30, 6, 14, 0.5, 7)
+    ex, cases = on_the_fly_cases(inst, costs)
+    assert len(cases) >= 3
+    found = 0
+    for k, cap in cases:
+        r = O.learn(inst, costs=costs, neg_type=1, max_cost=14, cache_rows=cap)
+        assert r.on_the_fly and r.num_rows == cap
+        assert np.array_equal(r.rows, ex.rows[:cap])
+        if r.status == O.FOUND:
+            found += 1
+            assert O.separates(r.formula, inst) and O.formula_cost(r.formula, costs) == r.cost >= ex.cost
+            assert r.cost <= k + 1 + last_round_gap(costs)
+        else:
+            assert r.status == O.NOT_FOUND and r.cost == k + 1 + last_round_gap(costs)
+    assert found >= 1

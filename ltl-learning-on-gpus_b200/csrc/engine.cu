@@ -1198,19 +1198,23 @@ LTLG_API int ltlg_device_apply_op(int32_t op, const uint64_t *a, const uint64_t 
 
 LTLG_API int ltlg_read_scarlet(const char *path, ltlg_traces *out) {
     memset(out, 0, sizeof(*out));
-    ScarletFile f;
-    if (!path || !read_scarlet(path, f)) return LTLG_BAD_ARGS;
-    std::vector<uint32_t> steps;
-    std::vector<int32_t> offsets;
-    std::string alpha;
-    scarlet_to_masks(f, steps, offsets, alpha);
+    ScarletMasks f;
+    if (!path || !read_scarlet_masks(path, f)) return LTLG_BAD_ARGS;
+    const std::vector<uint32_t> &steps = f.steps;
+    const std::vector<int32_t> &offsets = f.offsets;
     uint32_t *s = (uint32_t *)malloc(std::max<size_t>(steps.size(), 1) * 4);
     int32_t *o = (int32_t *)malloc(offsets.size() * 4);
-    char *a = strdup(alpha.c_str());
+    char *a = strdup(f.sorted_alphabet.c_str());
+    if (!s || !o || !a) {
+        free(s);
+        free(o);
+        free(a);
+        return LTLG_NO_MEMORY;
+    }
     if (!steps.empty()) memcpy(s, steps.data(), steps.size() * 4);
     memcpy(o, offsets.data(), offsets.size() * 4);
-    out->num_pos = (int32_t)f.pos.size();
-    out->num_neg = (int32_t)f.neg.size();
+    out->num_pos = f.num_pos;
+    out->num_neg = f.num_neg;
     out->alphabet = a;
     out->steps = s;
     out->offsets = o;

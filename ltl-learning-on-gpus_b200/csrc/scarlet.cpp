@@ -6,6 +6,8 @@
 // position, '1' adding the letter at that position.
 #include "scarlet.hpp"
 
+#include <cstdio>
+#include <cstring>
 #include <fstream>
 #include <iterator>
 #include <sstream>
@@ -80,6 +82,65 @@ void scarlet_to_masks(const ScarletFile &f, std::vector<uint32_t> &steps, std::v
             offsets.push_back((int32_t)steps.size());
         }
     }
+}
+
+bool read_scarlet_masks(const std::string &path, ScarletMasks &out) {
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) return false;
+    std::string text;
+    char buf[1 << 16];
+    for (size_t k; (k = fread(buf, 1, sizeof(buf), f)) > 0;) text.append(buf, k);
+    fclose(f);
+    // letters: the last line, one trailing newline ignored (as read_scarlet)
+    size_t end = text.size();
+    if (end && text[end - 1] == '\n') --end;
+    const size_t nl = text.rfind('\n', end ? end - 1 : 0);
+    const size_t first = (nl == std::string::npos || nl >= end) ? 0 : nl + 1;
+    std::vector<uint32_t> vbit;  // value position -> letter bit
+    uint32_t letters = 0;
+    for (size_t i = first; i < end; ++i) {
+        const char c = text[i];
+        if (c >= 'a' && c <= 'z') {
+            vbit.push_back(1u << (c - 'a'));
+            letters |= 1u << (c - 'a');
+        }
+    }
+    out.sorted_alphabet.clear();
+    for (int b = 0; b < 26; ++b)
+        if ((letters >> b) & 1u) out.sorted_alphabet += (char)('a' + b);
+    out.steps.clear();
+    out.offsets.assign(1, 0);
+    out.num_pos = out.num_neg = 0;
+    // trace lines: positives up to the first "---" line, negatives up to the next one;
+    // lines end at '\n' (a final line needs none, an empty segment after the last '\n' is
+    // not a line), and a separator is exactly "---"
+    const char *p = text.data(), *const e = p + text.size();
+    int side = 0;
+    while (p < e && side < 2) {
+        const char *q = static_cast<const char *>(memchr(p, '\n', (size_t)(e - p)));
+        if (!q) q = e;
+        if (q - p == 3 && p[0] == '-' && p[1] == '-' && p[2] == '-') {
+            ++side;
+        } else {
+            uint32_t m = 0;
+            size_t j = 0;
+            for (const char *c = p; c < q; ++c) {
+                if (*c == ';') {
+                    out.steps.push_back(m);
+                    m = 0;
+                    j = 0;
+                } else if (*c != ',') {
+                    if (*c == '1' && j < vbit.size()) m |= vbit[j];
+                    ++j;
+                }
+            }
+            out.steps.push_back(m);
+            out.offsets.push_back((int32_t)out.steps.size());
+            ++(side == 0 ? out.num_pos : out.num_neg);
+        }
+        p = q + 1;
+    }
+    return true;
 }
 
 }  // namespace ltlg

@@ -22,4 +22,14 @@ bool read_scarlet(const std::string &path, ScarletFile &out);
 void scarlet_to_masks(const ScarletFile &f, std::vector<uint32_t> &steps, std::vector<int32_t> &offsets,
                       std::string &sorted_alphabet);
 
+// The same file read in one pass straight to step masks, with no per-step strings: what
+// read_scarlet followed by scarlet_to_masks gives, for large trace files.
+struct ScarletMasks {
+    int32_t num_pos = 0, num_neg = 0;
+    std::string sorted_alphabet;
+    std::vector<uint32_t> steps;
+    std::vector<int32_t> offsets;  // num_pos + num_neg + 1 entries
+};
+bool read_scarlet_masks(const std::string &path, ScarletMasks &out);
+
 }  // namespace ltlg

@@ -57,13 +57,15 @@ class Instance:
         return out
 
     def trace_lines(self) -> list[str]:
-        """Scarlet lines ("1,0;0,1;...") in alphabet order, positives then negatives."""
-        lines = []
-        for t in range(self.n):
-            s = self.steps[self.offsets[t]:self.offsets[t + 1]]
-            lines.append(";".join(",".join("1" if (int(m) >> (ord(c) - 97)) & 1 else "0"
-                                           for c in self.alphabet) for m in s))
-        return lines
+        """Scarlet lines ("1,0;0,1;...") in alphabet order, positives then negatives.  Each
+        distinct step mask is formatted once."""
+        steps = np.asarray(self.steps, dtype=np.uint32)
+        bits = [1 << (ord(c) - 97) for c in self.alphabet]
+        masks, inv = np.unique(steps, return_inverse=True)
+        text = np.array([",".join("1" if int(m) & b else "0" for b in bits) for m in masks] or [""], dtype=object)
+        tokens = text[inv.ravel()].tolist()
+        offs = np.asarray(self.offsets).tolist()
+        return [";".join(tokens[offs[t]:offs[t + 1]]) for t in range(self.n)]
 
     def to_scarlet(self) -> str:
         """Same layout as the reference driver writes (code/dc.py:8-21)."""
@@ -274,7 +276,8 @@ def from_scarlet_text(text: str) -> Instance:
     advances the value index, '1' marking the letter at that index.
     """
     lines = text.split("\n")
-    last = ""
+    if lines and lines[-1] == "":
+        lines.pop()  # getline yields no line after a final newline
     body = text[:-1] if text.endswith("\n") else text
     k = body.rfind("\n")
     last = body[k + 1:] if k >= 0 else body

@@ -88,3 +88,56 @@ def test_one_shot_learn_checks_limits_before_the_device():
     assert res.status == api.INPUT_LIMITS and res.formula == "see_the_error" and res.cost == 2
     over = load_fixture("over64.trace")
     assert api.learn(over, limit_traces=True).status == api.INPUT_LIMITS
+
+
+def test_scarlet_reader_fuzz(tmp_path):
+    """The library's one-pass reader and the Python restatement agree on malformed files:
+    stray characters, carriage returns, empty lines, values beyond the alphabet, missing or
+    extra separators, no final newline."""
+    rng = np.random.default_rng(7)
+    parts = ["0", "1", "1", ",", ";", " ", "\r", "x", "\n"]
+    for case in range(300):
+        lines = []
+        for _ in range(int(rng.integers(0, 12))):
+            if rng.random() < 0.15:
+                lines.append("---")
+            else:
+                lines.append("".join(rng.choice(parts[:-1]) for _ in range(int(rng.integers(0, 14)))))
+        letters = "".join(rng.choice(list("abcdpqrz,; \r")) for _ in range(int(rng.integers(0, 8))))
+        text = "\n".join(lines + [letters]) + ("\n" if rng.random() < 0.5 else "")
+        p = tmp_path / f"f{case}.trace"
+        p.write_bytes(text.encode())
+        a = api.read_scarlet(str(p))
+        b = gen.from_scarlet_text(text)
+        assert (a.num_pos, a.num_neg, a.alphabet) == (b.num_pos, b.num_neg, b.alphabet), (case, text)
+        assert np.array_equal(a.offsets, b.offsets) and np.array_equal(a.steps, b.steps), (case, text)
+
+
+def test_scarlet_reader_large_file(tmp_path):
+    """A file of 50,000 + 50,000 traces of 10 steps over 4 letters (the shape of the
+    reference's largest Varying_size inputs) reads in well under a second."""
+    import time
+    rng = np.random.default_rng(1)
+    vals = rng.integers(0, 4, size=(100000, 10))
+    onehot = ["1,0,0,0", "0,1,0,0", "0,0,1,0", "0,0,0,1"]
+    lines = [";".join(onehot[v] for v in row) for row in vals]
+    text = "\n".join(lines[:50000] + ["---"] + lines[50000:] + ["---", "G,F,!,U,&,|,X", "---", "a,b,c,d"])
+    p = tmp_path / "nw50000.trace"
+    p.write_text(text)
+    t0 = time.perf_counter()
+    t = api.read_scarlet(str(p))
+    el = time.perf_counter() - t0
+    assert t.num_pos == 50000 and t.num_neg == 50000 and t.alphabet == "abcd"
+    assert np.array_equal(t.steps, (1 << vals.ravel()).astype(np.uint32))
+    assert el < 1.0, el
+
+
+def test_scarlet_writer_round_trip(tmp_path):
+    """Instance.to_scarlet (the layout of code/dc.py:8-21) read back by the library."""
+    for seed in range(4):
+        inst = gen.generate(seed, 3, 30, 25, 1, 20, 0.5, 5)
+        p = tmp_path / f"r{seed}.trace"
+        p.write_text(inst.to_scarlet())
+        t = api.read_scarlet(str(p))
+        assert (t.num_pos, t.num_neg, t.alphabet) == (inst.num_pos, inst.num_neg, inst.alphabet)
+        assert np.array_equal(t.offsets, inst.offsets) and np.array_equal(t.steps, inst.steps)

@@ -46,8 +46,9 @@ class Timeout(Exception):
 
 
 class Unsolvable(Exception):
-    """A sub-problem of at most one trace has no formula within the cost bound (the reference
-    recurses on it forever)."""
+    """A sub-problem of at most one trace has no formula within the cost bound, or the
+    recursion came back to a sub-problem it is still solving (e.g. one trace both positive
+    and negative).  The reference recurses on both forever."""
 
 
 class Driver:
@@ -65,6 +66,7 @@ class Driver:
         self._cache = {}
         self.deadline = deadline
         self.calls = 0
+        self._open = set()  # sub-problems on the recursion stack
 
     def _engine_solve(self, pos, neg):
         r = self.engine.learn(sub_instance(self.base, pos, neg), **self.opts)
@@ -91,8 +93,21 @@ class Driver:
         h = self._h(f)
         return [bool(h[self.base.num_pos + j]) for j in neg]
 
+    def _guarded(self, tag, step, window, pos, neg):
+        key = (tag, tuple(pos), tuple(neg))
+        if key in self._open:
+            raise Unsolvable()
+        self._open.add(key)
+        try:
+            return step(window, pos, neg)
+        finally:
+            self._open.discard(key)
+
     # ------------------------------------------------------------ DetSplit (dc.py:190-252)
     def det_split(self, window, pos, neg):
+        return self._guarded("det", self._det_split, window, pos, neg)
+
+    def _det_split(self, window, pos, neg):
         if len(pos) + len(neg) <= window:
             f = self.solve(pos, neg)
             if f is not None:
@@ -136,6 +151,9 @@ class Driver:
 
     # ------------------------------------------------------------ RandSplit (dc.py:255-327)
     def rand_split(self, window, pos, neg):
+        return self._guarded("rand", self._rand_split, window, pos, neg)
+
+    def _rand_split(self, window, pos, neg):
         rnd = random.Random(0)  # the reference reseeds at every call (dc.py:257)
         win = window
         while True:

@@ -110,3 +110,15 @@ def test_over_fitted_holds_exactly_on_the_positive_traces(seed):
     h = O.evaluate(f, inst)
     expect = np.array([ln in set(lines[:inst.num_pos]) for ln in lines], dtype=bool)
     assert np.array_equal(h.astype(bool), expect)
+
+
+@pytest.mark.parametrize("algo", ["det", "rand"])
+def test_contradictory_traces_end_as_unsolvable(algo):
+    """One trace both positive and negative: the recursion comes back to a sub-problem it is
+    still solving (the reference recurses until its timeout); the driver raises Unsolvable,
+    which run_dc reports as not_found."""
+    text = "1,0;0,1\n0,1\n---\n1,0;0,1\n---\nAll operators\n---\np,q"
+    inst = gen.from_scarlet_text(text)
+    d = _driver(inst)
+    with pytest.raises(divide.Unsolvable):
+        (d.rand_split if algo == "rand" else d.det_split)(4, [0, 1], [0])

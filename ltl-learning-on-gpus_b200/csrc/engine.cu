@@ -23,6 +23,7 @@
 #include "ltl_kernels.cuh"
 #include "ltlgpu.h"
 #include "scarlet.hpp"
+#include "traces.hpp"
 
 using namespace ltlg;
 
@@ -355,7 +356,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     const std::string alpha = t->alphabet ? t->alphabet : "";
     const int nalpha = (int)alpha.size();
     const bool ref_keys = opt->key_mode == LTLG_KEY_REF;
-    if (npos < 0 || nneg < 0 || (ref_keys && (opt->rlx_unq_chk_type < 1 || opt->rlx_unq_chk_type > 3)) ||
+    if (!traces_well_formed(t) || (ref_keys && (opt->rlx_unq_chk_type < 1 || opt->rlx_unq_chk_type > 3)) ||
         opt->key_mode < 0 || opt->key_mode > 2 || n > e->cfg.max_traces || nalpha > 26 ||
         (opt->order != LTLG_ORDER_PLAIN && opt->order != LTLG_ORDER_LEARNED) ||
         (opt->order == LTLG_ORDER_LEARNED && !e->has_scorer)) {
@@ -1026,6 +1027,12 @@ LTLG_API int ltlg_learn(const ltlg_traces *t, const ltlg_options *opt, ltlg_resu
     const int n = t ? t->num_pos + t->num_neg : 0;
     // The input limits are checked before the device is touched, as the reference checks
     // them before its first device call (ltli6463.cu:1078-1083).
+    if (t && opt && res && !traces_well_formed(t)) {
+        memset(res, 0, sizeof(*res));
+        res->status = LTLG_BAD_ARGS;
+        res->formula = strdup(ltlg_status_string(LTLG_BAD_ARGS));
+        return res->status;
+    }
     if (t && opt && res && t->offsets && t->num_pos >= 0 && t->num_neg >= 0) {
         int max_len = 0;
         for (int i = 0; i < n; ++i) max_len = std::max(max_len, t->offsets[i + 1] - t->offsets[i]);

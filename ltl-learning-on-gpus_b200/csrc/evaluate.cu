@@ -12,6 +12,7 @@
 
 #include "ltl_kernels.cuh"
 #include "ltlgpu.h"
+#include "traces.hpp"
 
 namespace ltlg {
 namespace {
@@ -89,7 +90,7 @@ struct DevMem {
 using namespace ltlg;
 
 extern "C" LTLG_API int ltlg_evaluate(const ltlg_traces *t, const char *formula, uint64_t *cs, uint8_t *holds) {
-    if (!t || !formula || t->num_pos < 0 || t->num_neg < 0) return LTLG_BAD_ARGS;
+    if (!formula || !traces_well_formed(t)) return LTLG_BAD_ARGS;
     const int n = t->num_pos + t->num_neg;
     const std::string alpha = t->alphabet ? t->alphabet : "";
     const std::string f = formula;

@@ -21,6 +21,7 @@
 
 #include "ltl_kernels.cuh"
 #include "ltlgpu.h"
+#include "traces.hpp"
 
 using namespace ltlg;
 
@@ -121,7 +122,7 @@ void write_node(const u64 *ent, int count, u64 parent, const char *alpha, int na
 
 extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_options *opt, char *formula,
                                            int32_t formula_cap, int32_t *cost_out, uint64_t *all_ltls_out) {
-    if (!t || !opt || !formula || formula_cap < 2) return LTLG_BAD_ARGS;
+    if (!t || !opt || !formula || formula_cap < 2 || !ltlg::traces_well_formed(t)) return LTLG_BAD_ARGS;
     formula[0] = 0;
     const int *cf = opt->cost_fun;
     for (int i = 0; i < 8; ++i)

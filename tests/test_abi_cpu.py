@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from ltlb200 import api, gen
 from helpers import fixture_path, load_fixture
@@ -141,3 +142,31 @@ def test_scarlet_writer_round_trip(tmp_path):
         t = api.read_scarlet(str(p))
         assert (t.num_pos, t.num_neg, t.alphabet) == (inst.num_pos, inst.num_neg, inst.alphabet)
         assert np.array_equal(t.offsets, inst.offsets) and np.array_equal(t.steps, inst.steps)
+
+
+def _raw(alphabet="pq", offsets=(0, 2, 3), steps=(1, 2, 3)):
+    return gen.Instance(1, 1, alphabet, np.array(steps, dtype=np.uint32), np.array(offsets, dtype=np.int32))
+
+
+def test_malformed_traces_are_refused_before_the_device():
+    """Decreasing or negative offsets and letters outside a-z would become negative shift
+    counts; every entry point that reads traces refuses them with LTLG_BAD_ARGS before it
+    looks for a device."""
+    good = _raw()
+    bad = [_raw(offsets=(0, 3, 2)), _raw(offsets=(-1, 1, 2)), _raw(alphabet="pQ"), _raw(alphabet="p1")]
+    L = api.lib()
+    f = L.ltlg_learn_noalloc
+    f.argtypes = [ctypes.POINTER(api.Traces), ctypes.POINTER(api.Options), ctypes.c_char_p, ctypes.c_int32,
+                  ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_uint64)]
+    f.restype = ctypes.c_int
+    for inst in bad:
+        r = api.learn(inst)
+        assert r.status == api.BAD_ARGS and r.formula == "bad_arguments"
+        with pytest.raises(ValueError, match="bad_arguments"):
+            api.evaluate(inst, "p")
+        t, keep = api._traces(inst)
+        o = api.make_options()
+        buf = ctypes.create_string_buffer(64)
+        assert f(ctypes.byref(t), ctypes.byref(o), buf, 64, None, None) == api.BAD_ARGS
+    # a well-formed set gets past the checks to the device lookup
+    assert api.learn(good).status != api.BAD_ARGS

@@ -4,7 +4,6 @@ the sum of the units over ranks."""
 import os
 import socket
 
-import pytest
 import torch.multiprocessing as mp
 
 

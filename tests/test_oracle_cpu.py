@@ -221,3 +221,43 @@ def test_oracle_on_the_fly_regime(costs):
         else:
             assert r.status == O.NOT_FOUND and r.cost == k + 1 + last_round_gap(costs)
     assert found >= 1
+
+
+def _edge(pos_steps, neg_steps, alphabet="pq"):
+    """An instance from explicit step masks (lists of lists of ints), empty traces allowed."""
+    traces = list(pos_steps) + list(neg_steps)
+    offs = np.zeros(len(traces) + 1, dtype=np.int32)
+    for i, t in enumerate(traces):
+        offs[i + 1] = offs[i] + len(t)
+    steps = np.array([m for t in traces for m in t], dtype=np.uint32)
+    return gen.Instance(len(pos_steps), len(neg_steps), alphabet, steps, offs)
+
+
+P, Q = 1 << (ord("p") - 97), 1 << (ord("q") - 97)
+EDGE = {
+    "no_negatives": _edge([[P, Q], [P | Q]], []),
+    "no_positives": _edge([], [[P], [Q, 0, P]]),
+    "empty_trace": _edge([[P, 0, Q]], [[], [Q]]),
+    "one_step_traces": _edge([[P], [P | Q]], [[Q], [0]]),
+    "max_length_trace": _edge([[P if k % 3 else Q for k in range(63)]], [[Q] * 63, [P] * 5]),
+    "duplicate_traces": _edge([[P, Q], [P, Q]], [[Q, P], [Q, P]]),
+    "contradiction": _edge([[P, Q]], [[P, Q]]),
+}
+
+
+@pytest.mark.parametrize("name", sorted(EDGE))
+def test_oracle_edge_cases_equal_brute_force(name):
+    """Inputs at the domain's edges: an empty side, a trace of no steps, one-step traces, a
+    trace of the maximum 63 steps, duplicate traces, and one trace on both sides."""
+    inst = EDGE[name]
+    costs = [1] * 8
+    want = brute_force_levels(inst, costs, 4, 1)
+    run = O.learn(inst, costs=costs, max_cost=4, neg_type=1, stop_at_found=False)
+    for c in range(1, 5):
+        assert run.level_set(c) == want[c], (name, c)
+    found = O.learn(inst, costs=costs, max_cost=4, neg_type=1)
+    if name == "contradiction":
+        assert found.status == O.NOT_FOUND and found.formula == "not_found"
+    else:
+        assert found.status == O.FOUND and O.separates(found.formula, inst), name
+        assert O.formula_cost(found.formula) == found.cost

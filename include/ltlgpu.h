@@ -92,7 +92,9 @@ typedef struct ltlg_engine_config {
 
 typedef struct ltlg_options {
     int32_t cost_fun[8];       /* p ~ & | X F G U, each in 1..SHRT_MAX */
-    int32_t max_cost;
+    int32_t max_cost;          /* levels up to min(max_cost, 511) are enumerated (the device keeps
+                                  511 level starts); a search that reaches 511 without a find
+                                  ends NOT_FOUND with cost 511 */
     int32_t rlx_unq_chk_type;  /* the reference's argument 11 (1, 2, 3), used with LTLG_KEY_REF */
     int32_t neg_type;          /* 1: negate every formula, 2: negate letters only (ltli6463.cu:1212) */
     int32_t key_mode;          /* ltlg_key_mode */

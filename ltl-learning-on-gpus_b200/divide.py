@@ -57,7 +57,7 @@ class Driver:
     formula holds at position 0 (positives first).  By default both run on the device."""
 
     def __init__(self, base: Instance, engine: api.Engine | None = None, solve=None, holds=None,
-                 costs=(1,) * 8, max_cost=500, rlx_type=3, neg_type=2, key_mode=api.KEY_REF, deadline=None):
+                 costs=(1,) * 8, max_cost=500, rlx_type=3, neg_type=2, key_mode=api.KEY_EXACT, deadline=None):
         self.base = base
         self.engine = engine
         self.opts = dict(costs=costs, max_cost=max_cost, rlx_type=rlx_type, neg_type=neg_type, key_mode=key_mode)

@@ -261,3 +261,18 @@ def test_oracle_edge_cases_equal_brute_force(name):
     else:
         assert found.status == O.FOUND and O.separates(found.formula, inst), name
         assert O.formula_cost(found.formula) == found.cost
+
+
+@pytest.mark.parametrize("case", range(12))
+def test_oracle_levels_equal_brute_force_random_costs(case):
+    """Seeded cost functions (each operator 1-3, letters 1-2) and both NegTypes on small
+    instances: the split rule, the NegType rule and the level order under uneven costs."""
+    rng = np.random.default_rng(1000 + case)
+    costs = [int(rng.integers(1, 3))] + [int(c) for c in rng.integers(1, 4, size=7)]
+    neg_type = 1 + case % 2
+    inst = gen.generate(30 + case, 2, 3, 3, 2, 5, 0.5, 3)
+    max_cost = costs[0] + 5
+    want = brute_force_levels(inst, costs, max_cost, neg_type)
+    run = O.learn(inst, costs=costs, max_cost=max_cost, neg_type=neg_type, stop_at_found=False)
+    for c in range(costs[0], max_cost + 1):
+        assert run.level_set(c) == want.get(c, set()), (costs, neg_type, c)

@@ -276,3 +276,54 @@ def test_oracle_levels_equal_brute_force_random_costs(case):
     run = O.learn(inst, costs=costs, max_cost=max_cost, neg_type=neg_type, stop_at_found=False)
     for c in range(costs[0], max_cost + 1):
         assert run.level_set(c) == want.get(c, set()), (costs, neg_type, c)
+
+
+def py_ref_key(cs, lens, rtype):
+    """The reference's 126-bit keys (ltli6463.cu:57-141) restated as a list of chosen (trace,
+    bit) positions, of which the first 126 are packed: bits 0-62 into l, 63-125 into h.  Exact
+    packing when lenSum <= 126; else type 1 samples every (lenSum // 126)-th step, type 2
+    takes the first (126 len + lenSum) // lenSum steps of each trace, and type 3 XORs the
+    splitmix64 finaliser of every word into h (first half of the traces) or l."""
+    n, lensum, mask = len(cs), int(sum(lens)), (1 << 64) - 1
+    if lensum > 126 and rtype == 3:
+        h = l = 0
+        for i, w in enumerate(cs):
+            x = int(w)
+            x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & mask
+            x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & mask
+            x ^= x >> 31
+            if i < n // 2:
+                h ^= x
+            else:
+                l ^= x
+        return h, l
+    picks = []
+    for i in range(n):
+        if lensum <= 126:
+            ks = range(int(lens[i]))
+        elif rtype == 1:
+            ks = range(0, int(lens[i]), lensum // 126)
+        else:
+            ks = range((126 * int(lens[i]) + lensum) // lensum)
+        picks += [(i, k) for k in ks]
+    h = l = 0
+    for j, (i, k) in enumerate(picks[:126]):
+        if k < 64 and (int(cs[i]) >> k) & 1:
+            if j < 63:
+                l |= 1 << j
+            else:
+                h |= 1 << (j - 63)
+    return h, l
+
+
+@pytest.mark.parametrize("rtype", [1, 2, 3])
+def test_reference_keys_bit_for_bit(rtype):
+    rng = np.random.default_rng(rtype)
+    for trial in range(300):
+        n = int(rng.integers(1, 40))
+        lens = rng.integers(0 if trial % 7 == 0 else 1, 64, size=n)
+        if trial % 3 == 0:  # the exact-pack regime
+            lens = np.minimum(lens, 126 // n)
+        words = rng.integers(0, 1 << 63, size=n, dtype=np.uint64) * np.uint64(2) + rng.integers(0, 2, size=n).astype(np.uint64)
+        cs = words & ((np.uint64(1) << lens.astype(np.uint64)) - np.uint64(1))
+        assert O.ref_key(cs, lens, rtype) == py_ref_key(cs, lens, rtype), (rtype, trial, lens.tolist())

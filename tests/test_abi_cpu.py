@@ -170,3 +170,16 @@ def test_malformed_traces_are_refused_before_the_device():
         assert f(ctypes.byref(t), ctypes.byref(o), buf, 64, None, None) == api.BAD_ARGS
     # a well-formed set gets past the checks to the device lookup
     assert api.learn(good).status != api.BAD_ARGS
+
+
+def test_generate_many_in_child_interpreters_equals_sequential():
+    """The parallel generator (child interpreters, chunks of specs) gives the sequential
+    instances, in order."""
+    from ltlb200 import workloads
+    specs = list(workloads.cfg4_specs(10, seed=3))
+    par = list(workloads.generate_many("generate", specs, workers=3, chunk=4))
+    seq = [gen.generate(*s) for s in specs]
+    assert len(par) == len(seq) == 10
+    for a, b in zip(par, seq):
+        assert (a.num_pos, a.num_neg, a.alphabet, a.hidden) == (b.num_pos, b.num_neg, b.alphabet, b.hidden)
+        assert np.array_equal(a.steps, b.steps) and np.array_equal(a.offsets, b.offsets)

@@ -392,8 +392,9 @@ def run_ours(a):
                          "alg_bytes_per_launch": alg_bytes / nl,
                          "kernel": "level_kernel", "bytes_per_unit": per_unit,
                          "units": "candidates evaluated + uniques stored",
-                         "timing": "level time from CUDA events on the engine stream (planner + level kernel "
-                                   "+ 2 small D2H copies per level), summed over the one-at-a-time pass",
+                         "timing": "level time from CUDA events on the engine stream around each level's graph "
+                                   "(planner + level kernel; the kernel writes the level summary into mapped "
+                                   "host memory), summed over the one-at-a-time pass",
                          "traffic_source": "ncu DRAM bytes per candidate of the cost-8 level_kernel launch "
                                            "(profiles/level_kernel_cfg2.txt) x mean candidates per launch"},
             "gpu_launches": launches,

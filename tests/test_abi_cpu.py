@@ -183,3 +183,21 @@ def test_generate_many_in_child_interpreters_equals_sequential():
     for a, b in zip(par, seq):
         assert (a.num_pos, a.num_neg, a.alphabet, a.hidden) == (b.num_pos, b.num_neg, b.alphabet, b.hidden)
         assert np.array_equal(a.steps, b.steps) and np.array_equal(a.offsets, b.offsets)
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/ltlgpu.h compiles as C99 (-pedantic, warnings as errors) and a C program links
+    against the library and calls it: the boundary needs no C++ on the caller's side."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "c_abi.c"
+    src.write_text('#include "ltlgpu.h"\n'
+                   "int main(void) { ltlg_options o; ltlg_default_options(&o);\n"
+                   "  return (o.max_cost == 500 && ltlg_abi_version() == 1) ? 0 : 1; }\n")
+    lib_dir = os.path.dirname(api.LIB_PATH)
+    exe = tmp_path / "c_abi"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-L", lib_dir, "-lltlgpu", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
+    assert subprocess.run([str(exe)]).returncode == 0

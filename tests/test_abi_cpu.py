@@ -201,3 +201,29 @@ def test_header_is_plain_c(tmp_path):
     subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
                     str(src), "-L", lib_dir, "-lltlgpu", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
     assert subprocess.run([str(exe)]).returncode == 0
+
+
+def test_null_handles_and_no_device():
+    """Accessors and destructors accept null handles; creating an engine or a batch on a host
+    without a CUDA device returns LTLG_NO_DEVICE and no handle (no CPU fallback)."""
+    if _has_cuda():
+        pytest.skip("checks the no-device path")
+    L = api.lib()
+    assert L.ltlg_engine_stream(None) is None and L.ltlg_batch_stream(None, 0) is None
+    L.ltlg_engine_destroy(None)
+    L.ltlg_batch_destroy(None)
+    L.ltlg_result_free(None)
+    L.ltlg_traces_free(None)
+    cfg = api.EngineConfig()
+    L.ltlg_default_engine_config(ctypes.byref(cfg))
+    h = ctypes.c_void_p()
+    assert L.ltlg_engine_create(ctypes.byref(cfg), ctypes.byref(h)) == api.NO_DEVICE and not h.value
+    assert L.ltlg_batch_create(ctypes.byref(cfg), 2, ctypes.byref(h)) == api.NO_DEVICE and not h.value
+
+
+def _has_cuda():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False

@@ -152,6 +152,9 @@ LTLG_API void ltlg_default_engine_config(ltlg_engine_config *cfg);
 /* The reference's defaults: unit costs, maxCost 500, type 3, NegType 2, exact keys, fused, plain. */
 LTLG_API void ltlg_default_options(ltlg_options *opt);
 
+/* A handle owning one device's buffers and stream (the reference allocates and frees its
+ * device memory inside every LTLI call, ltli6463.cu:1152-1190, :1487-1493).  Without a CUDA
+ * device: LTLG_NO_DEVICE and no handle.  Destroy accepts NULL. */
 LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg, ltlg_engine **out);
 LTLG_API void ltlg_engine_destroy(ltlg_engine *eng);
 
@@ -163,9 +166,15 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *eng, const ltlg_traces *traces, cons
  * learns with their own events. */
 LTLG_API void *ltlg_engine_stream(ltlg_engine *eng);
 
-/* One-shot form: creates an engine sized for the input, learns, destroys it. */
+/* One-shot form, the reference's LTLI (ltli6463.cu:1043-1052) call for call: creates an
+ * engine sized for the input, learns, destroys it.  Malformed traces (LTLG_BAD_ARGS) and
+ * the input limits (LTLG_INPUT_LIMITS, ltli6463.cu:1078-1083) are reported before any
+ * device call. */
 LTLG_API int ltlg_learn(const ltlg_traces *traces, const ltlg_options *opt, ltlg_result *res);
 
+/* Frees the strings and arrays of a result (the reference returns std::string; its sentinel
+ * strings "not_found", "see_the_error", "Size of the output is too big" are statuses and
+ * formula text here, ltli6463.cu:1461, :1082, :984).  Accepts NULL. */
 LTLG_API void ltlg_result_free(ltlg_result *res);
 
 /* Batched learning: independent instances spread over `workers` engines (each with its own

@@ -111,6 +111,9 @@ int main(int argc, char *argv[]) {
         return 0;
     }
     if (progress) {
+        // the letters' line, printed by the reference before its first level (ltli6463.cu:1095-1098)
+        printf("Cost %-2d | (A) | AllLTLs: %-11lu | StoredLTLs: %-10d | ToBeChecked: %-10d \n", opt.cost_fun[0], 0ul,
+               0, (int)alpha.size());
         for (int b = 0; b < res.num_blocks; ++b) {
             const ltlg_block_stat &s = res.blocks[b];
             static const char ops[] = "~&|XFGU";

@@ -119,3 +119,25 @@ def test_stdout_layout_without_a_device(name):
     assert rest[4].startswith("Cost of Final LTL: ")
     assert rest[5].startswith("Running Time: ") and rest[5].endswith(" s")
     assert out.split("\n")[-2] == 'LTL: "no_cuda_device"'
+
+
+def test_per_block_letters_line_matches_reference_runs():
+    """With --per-block the first line is the letters' progress line, as the reference binary
+    printed it in every recorded run (ltli6463.cu:1095-1098; printed before any device work)."""
+    from helpers import reference_runs
+    runs = reference_runs()
+    if runs is None:
+        pytest.skip("reference outputs not recorded")
+    seen = 0
+    for r in runs["runs"]:
+        if r["final"]["limits_error"]:
+            continue
+        cost, op, all_before, stored, to_check = r["progress"][0]
+        assert op == "A"
+        p = subprocess.run([CLI, fixture_path(r["file"]), *[str(c) for c in r["costs"]], str(r["max_cost"]),
+                            str(r["rlx"]), str(r["neg"]), "--per-block"], capture_output=True, text=True, timeout=300)
+        first = p.stdout.split("\n")[0]
+        assert first == (f"Cost {cost:<2d} | (A) | AllLTLs: {all_before:<11d} | StoredLTLs: {stored:<10d} | "
+                         f"ToBeChecked: {to_check:<10d} "), (r["id"], first)
+        seen += 1
+    assert seen >= 70

@@ -37,7 +37,7 @@ extern "C" {
 #endif
 
 #define LTLG_API __attribute__((visibility("default")))
-#define LTLG_ABI_VERSION 1
+#define LTLG_ABI_VERSION 2
 
 typedef struct ltlg_traces {
     int32_t num_pos;
@@ -73,8 +73,15 @@ enum ltlg_status {
     LTLG_CUDA_ERROR = 6,
     LTLG_DEVICE_WAIT = 7,      /* a bounded device-side wait gave up; results are not trusted */
     LTLG_TABLE_FULL = 8,
-    LTLG_NO_DEVICE = 9
+    LTLG_NO_DEVICE = 9,
+    LTLG_FORMULA_TOO_LONG = 10 /* the formula does not fit the caller's buffer (ltlg_learn_noalloc) */
 };
+
+/* Bytes that always hold a returned formula and its NUL.  The reference prints "Size of the
+ * output is too big" once the found formula has more than 199 operator nodes below its root
+ * (its 600-int index buffer, ltli6463.cu:959-985); 200 binary nodes and 201 letters make 1,201
+ * characters. */
+#define LTLG_FORMULA_MAX_BYTES 1280
 
 typedef struct ltlg_engine_config {
     int32_t device;            /* CUDA device ordinal */
@@ -88,6 +95,13 @@ typedef struct ltlg_engine_config {
     int32_t unary_rows;        /* source rows per unary work item */
     int32_t small_rows;        /* levels below the small-level size: right rows (unary: source-row
                                   pairs) per warp and work item; 0 = 1 */
+    int32_t wait_spins;        /* bound of a device wait for another warp's hash-slot publication, in
+                                  polls about 128 ns apart; a wait that runs out ends the learn with
+                                  LTLG_DEVICE_WAIT.  0 = 2^22 (about half a second) */
+    int32_t pad_;
+    int64_t small_level;       /* levels with fewer candidates are cut into work items of one right row
+                                  (unary: one source row) per warp; larger levels use right_chunk /
+                                  unary_rows.  0 = 2048 x the level kernel's resident CTAs */
 } ltlg_engine_config;
 
 typedef struct ltlg_options {
@@ -147,7 +161,7 @@ typedef struct ltlg_result {
 typedef struct ltlg_engine ltlg_engine;
 
 /* Defaults: device 0, 2^27 slots, 16 GiB cache, n <= 8192, 256 threads, left tile 4,
-   right chunk 16, unary rows 32, small rows 1. */
+   right chunk 16, unary rows 32, small rows 1, default wait bound and small-level size. */
 LTLG_API void ltlg_default_engine_config(ltlg_engine_config *cfg);
 /* The reference's defaults: unit costs, maxCost 500, type 3, NegType 2, exact keys, fused, plain. */
 LTLG_API void ltlg_default_options(ltlg_options *opt);
@@ -194,12 +208,14 @@ LTLG_API void *ltlg_batch_stream(ltlg_batch *b, int32_t worker);
  * allocate device memory (GPU memory owned by another allocator, or no cudaMalloc allowed
  * after start-up): every device buffer lives in one static 64 MiB array that the library
  * holds on each GPU until exit, and host work uses stack arrays.  At most 64 traces of at
- * most 63 steps (more: LTLG_INPUT_LIMITS); exact or 64-bit-fingerprint keys; a level that
- * overflows the scratch returns LTLG_NO_MEMORY.  The formula is written to the caller's
- * buffer (formula_cap bytes), the cost and candidate count to *cost and *all_ltls.  All
- * calls share the array: calls whose GPU work overlaps race, so callers serialise them.
- * The first call on a device looks up the array's address there; make it before any
- * stream capture. */
+ * most 63 steps (more: LTLG_INPUT_LIMITS); exact or 64-bit-fingerprint keys; max_cost below
+ * 512; a level that overflows the scratch returns LTLG_NO_MEMORY.  The formula is written to
+ * the caller's buffer (formula_cap bytes, at least 16; LTLG_FORMULA_MAX_BYTES always
+ * suffices), the cost and candidate count to *cost and *all_ltls.  A formula (or the
+ * reference's "Size of the output is too big") that does not fit returns
+ * LTLG_FORMULA_TOO_LONG with an empty string and *cost and *all_ltls set.  All calls share
+ * the array: calls whose GPU work overlaps race, so callers serialise them.  The first call
+ * on a device looks up the array's address there; make it before any stream capture. */
 LTLG_API int ltlg_learn_noalloc(const ltlg_traces *traces, const ltlg_options *opt, char *formula,
                                 int32_t formula_cap, int32_t *cost, uint64_t *all_ltls);
 
@@ -210,6 +226,13 @@ LTLG_API int ltlg_engine_read_rows(ltlg_engine *eng, int64_t first, int64_t coun
                                    uint64_t *parents);
 /* Row ranges of each cost after a learn: starts[c] for c in 0..max_cost + 1. */
 LTLG_API int ltlg_engine_level_starts(ltlg_engine *eng, int64_t *starts, int32_t count);
+
+/* Fault injection for tests (no counterpart in the reference).  Marks the hash-set slot of the
+ * CS `cs` (n words, exact keys) as "publication pending" for the engine's next learn: the first
+ * candidate of that learn with this CS waits for a publication that never comes, gives up after
+ * wait_spins polls and the learn returns LTLG_DEVICE_WAIT.  The mark belongs to one hash-set
+ * generation, so the learn after that one starts clean.  Returns 0 or an ltlg_status. */
+LTLG_API int ltlg_engine_hold_slot(ltlg_engine *eng, const uint64_t *cs, int32_t n);
 
 /* Device building blocks, for kernel-level parity tests (device buffers are allocated
  * and freed inside; host arrays in and out). */

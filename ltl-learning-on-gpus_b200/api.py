@@ -17,11 +17,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libltlgpu.so")
 CLI_PATH = os.path.join(HERE, "_build", "ltli6463")
 
+ABI_VERSION = 2  # LTLG_ABI_VERSION of include/ltlgpu.h
 KEY_EXACT, KEY_REF, KEY_HASH64 = 0, 1, 2
 SCHEDULE_FUSED, SCHEDULE_PER_BLOCK = 0, 1
 ORDER_PLAIN, ORDER_LEARNED = 0, 1
 (FOUND, NOT_FOUND, INPUT_LIMITS, TIMEOUT, NO_MEMORY, BAD_ARGS, CUDA_ERROR, DEVICE_WAIT, TABLE_FULL,
- NO_DEVICE) = range(10)
+ NO_DEVICE, FORMULA_TOO_LONG) = range(11)
+FORMULA_MAX_BYTES = 1280
 OPS = "~&|XFGU"
 
 EXPORTED = [
@@ -31,7 +33,7 @@ EXPORTED = [
     "ltlg_traces_free", "ltlg_engine_stream", "ltlg_batch_create", "ltlg_batch_destroy", "ltlg_batch_learn",
     "ltlg_batch_stream", "ltlg_learn_noalloc", "ltlg_block_features", "ltlg_engine_set_scorer",
     "ltlg_batch_set_scorer", "ltlg_engine_label_blocks", "ltlg_scorer_forward", "ltlg_scorer_grad",
-    "ltlg_scorer_train", "ltlg_evaluate",
+    "ltlg_scorer_train", "ltlg_evaluate", "ltlg_engine_hold_slot",
 ]
 SCORER_FEATURES = 32
 SCORER_PARAMS = 6337
@@ -46,7 +48,8 @@ class EngineConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("slots_log2", C.c_int32), ("cache_bytes", C.c_int64),
                 ("max_rows", C.c_int64), ("max_traces", C.c_int32), ("block_threads", C.c_int32),
                 ("left_tile", C.c_int32), ("right_chunk", C.c_int32), ("unary_rows", C.c_int32),
-                ("small_rows", C.c_int32)]
+                ("small_rows", C.c_int32), ("wait_spins", C.c_int32), ("pad_", C.c_int32),
+                ("small_level", C.c_int64)]
 
 
 class Options(C.Structure):
@@ -140,6 +143,7 @@ def lib():
         L.ltlg_scorer_grad.argtypes = [fp, fp, fp, C.c_int32, C.c_float, fp, fp]
         L.ltlg_scorer_train.argtypes = [fp, fp, fp, C.c_int32, C.POINTER(TrainConfig), fp]
         L.ltlg_evaluate.argtypes = [C.POINTER(Traces), C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint8)]
+        L.ltlg_engine_hold_slot.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.c_int32]
         _lib = L
     return _lib
 
@@ -218,13 +222,11 @@ class Engine:
     """Device state for repeated learns: language cache, hash set, stream."""
 
     def __init__(self, device=0, slots_log2=27, cache_bytes=16 << 30, max_rows=64 << 20, max_traces=8192,
-                 block_threads=256, left_tile=4, right_chunk=16, unary_rows=32, small_rows=1):
+                 block_threads=256, left_tile=4, right_chunk=16, unary_rows=32, small_rows=1, wait_spins=0,
+                 small_level=0):
         L = lib()
-        cfg = EngineConfig()
-        L.ltlg_default_engine_config(C.byref(cfg))
-        cfg.device, cfg.slots_log2, cfg.cache_bytes, cfg.max_rows = device, slots_log2, cache_bytes, max_rows
-        cfg.max_traces, cfg.block_threads, cfg.left_tile = max_traces, block_threads, left_tile
-        cfg.right_chunk, cfg.unary_rows, cfg.small_rows = right_chunk, unary_rows, small_rows
+        cfg = _engine_config(device, slots_log2, cache_bytes, max_rows, max_traces, block_threads, left_tile,
+                             right_chunk, unary_rows, small_rows, wait_spins, small_level)
         h = C.c_void_p()
         rc = L.ltlg_engine_create(C.byref(cfg), C.byref(h))
         if rc != 0:
@@ -301,6 +303,14 @@ class Engine:
                              candidates=x.candidates, won=x.won))
         return out, meta, feats, won
 
+    def hold_slot(self, cs: np.ndarray):
+        """Fault injection for tests: the next learn finds the hash slot of this CS (exact keys)
+        held by a publication that never comes, so its wait runs out (DEVICE_WAIT)."""
+        a = np.ascontiguousarray(cs, dtype=np.uint64)
+        rc = lib().ltlg_engine_hold_slot(self._h, _u64p(a), a.size)
+        if rc != 0:
+            raise RuntimeError(f"hold_slot failed: {status_string(rc)}")
+
     def level_starts(self, count: int) -> list:
         a = (C.c_int64 * count)()
         lib().ltlg_engine_level_starts(self._h, a, count)
@@ -316,12 +326,14 @@ class Engine:
 
 
 def _engine_config(device=0, slots_log2=27, cache_bytes=16 << 30, max_rows=64 << 20, max_traces=8192,
-                   block_threads=256, left_tile=4, right_chunk=16, unary_rows=32, small_rows=1) -> EngineConfig:
+                   block_threads=256, left_tile=4, right_chunk=16, unary_rows=32, small_rows=1, wait_spins=0,
+                   small_level=0) -> EngineConfig:
     cfg = EngineConfig()
     lib().ltlg_default_engine_config(C.byref(cfg))
     cfg.device, cfg.slots_log2, cfg.cache_bytes, cfg.max_rows = device, slots_log2, cache_bytes, max_rows
     cfg.max_traces, cfg.block_threads, cfg.left_tile = max_traces, block_threads, left_tile
     cfg.right_chunk, cfg.unary_rows, cfg.small_rows = right_chunk, unary_rows, small_rows
+    cfg.wait_spins, cfg.small_level = wait_spins, small_level
     return cfg
 
 

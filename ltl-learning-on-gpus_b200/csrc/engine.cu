@@ -60,6 +60,28 @@ double now_s() {
 
 const char OPCH[7] = {'~', '&', '|', 'X', 'F', 'G', 'U'};
 
+u64 host_fmix64(u64 x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+// The level kernel's exact-key fingerprint of a CS (n words, zero padding up to pitch): word i
+// adds (lo(w) + lo(k)) * (hi(w) + hi(k)) with k = (i + 1) * 0x9E3779B97F4A7C15 (32-bit sums,
+// 64-bit product), and the sum goes through fmix64.  The device adds the same terms in
+// another order; the sum is the same modulo 2^64.
+u64 host_fingerprint_exact(const uint64_t *w, int n, int pitch) {
+    u64 sum = 0;
+    for (int i = 0; i < pitch; ++i) {
+        const u64 v = i < n ? w[i] : 0ull, k = (u64)(i + 1) * 0x9E3779B97F4A7C15ull;
+        sum += (u64)((u32)v + (u32)k) * (u64)((u32)(v >> 32) + (u32)(k >> 32));
+    }
+    return host_fmix64(sum);
+}
+
 }  // namespace
 
 struct ltlg_engine {
@@ -210,6 +232,7 @@ LTLG_API const char *ltlg_status_string(int s) {
     case LTLG_DEVICE_WAIT: return "device_wait_gave_up";
     case LTLG_TABLE_FULL: return "hash_set_full";
     case LTLG_NO_DEVICE: return "no_cuda_device";
+    case LTLG_FORMULA_TOO_LONG: return "formula_too_long";
     default: return "unknown";
     }
 }
@@ -226,6 +249,8 @@ LTLG_API void ltlg_default_engine_config(ltlg_engine_config *c) {
     c->right_chunk = 16;
     c->unary_rows = 32;
     c->small_rows = 1;
+    c->wait_spins = 0;
+    c->small_level = 0;
 }
 
 LTLG_API void ltlg_default_options(ltlg_options *o) {
@@ -253,7 +278,9 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
     if (cfg.slots_log2 < 10 || cfg.slots_log2 > 34) return LTLG_BAD_ARGS;
     if (cfg.left_tile != 2 && cfg.left_tile != 4 && cfg.left_tile != 8) return LTLG_BAD_ARGS;
     if (cfg.block_threads < 32 || cfg.block_threads > 256 || cfg.block_threads % 32) return LTLG_BAD_ARGS;
-    if (cfg.right_chunk < 1 || cfg.unary_rows < 1 || cfg.max_traces < 1) return LTLG_BAD_ARGS;
+    if (cfg.right_chunk < 1 || cfg.unary_rows < 1 || cfg.max_traces < 1 || cfg.wait_spins < 0 ||
+        cfg.small_level < 0)
+        return LTLG_BAD_ARGS;
     if (cfg.max_rows <= 0 || cfg.max_rows > (1ll << 30) - 1) cfg.max_rows = (1ll << 30) - 1;
     auto *e = new ltlg_engine();
     e->cfg = cfg;
@@ -527,8 +554,9 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     for (int i = 0; i < 8; ++i) A.cf[i] = cf[i];
     A.right_chunk_big = e->cfg.right_chunk;
     A.unary_rows_big = e->cfg.unary_rows;
-    A.small_level = max_grid * 2048ll;
+    A.small_level = e->cfg.small_level > 0 ? e->cfg.small_level : max_grid * 2048ll;
     A.small_rows = std::max(1, e->cfg.small_rows);
+    A.wait_spins = e->cfg.wait_spins > 0 ? e->cfg.wait_spins : (1ll << 22);
     A.hash_kind = hk;
     A.cap_rows = cap_rows;
     A.cache = (u64 *)e->cache.p;
@@ -1155,6 +1183,25 @@ LTLG_API int ltlg_engine_level_starts(ltlg_engine *e, int64_t *starts, int32_t c
     for (int32_t i = 0; i < count; ++i)
         starts[i] = i < (int32_t)e->level_start.size() ? e->level_start[i] : (e->level_start.empty() ? 0 : e->level_start.back());
     return 0;
+}
+
+LTLG_API int ltlg_engine_hold_slot(ltlg_engine *e, const uint64_t *cs, int32_t n) {
+    if (!e || !cs || n <= 0 || n > e->cfg.max_traces) return LTLG_BAD_ARGS;
+    cudaError_t err = cudaSetDevice(e->cfg.device);
+    if (err != cudaSuccess) return fail_cuda(e, err, nullptr);
+    const int pitch = std::max(4, (n + 3) & ~3);
+    const u64 fp = host_fingerprint_exact(cs, n, pitch);
+    if (e->gen >= 255) {  // the next learn would clear the set; clear it here instead
+        err = cudaMemsetAsync(e->slots.p, 0, e->nslots * 8, e->stream);
+        if (err != cudaSuccess) return fail_cuda(e, err, nullptr);
+        e->gen = 0;
+    }
+    // tag | the next learn's generation | "publication pending"
+    const u64 v = ((fp >> 40) << 40) | ((u64)(e->gen + 1) << 32) | 0xFFFFFFFFull;
+    u64 *slot = (u64 *)e->slots.p + (fp & (e->nslots - 1));
+    err = cudaMemcpyAsync(slot, &v, sizeof(v), cudaMemcpyHostToDevice, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    return err == cudaSuccess ? 0 : fail_cuda(e, err, nullptr);
 }
 
 LTLG_API int ltlg_device_apply_op(int32_t op, const uint64_t *a, const uint64_t *b, const uint64_t *lenmask,

@@ -36,7 +36,6 @@ constexpr u64 M63 = 0x7FFFFFFFFFFFFFFFull;
 constexpr u32 FIELD_PENDING = 0xFFFFFFFFu;
 constexpr u32 FIELD_OVERFLOW = 0xFFFFFFFEu;
 constexpr unsigned FULL = 0xFFFFFFFFu;
-constexpr long long WAIT_SPINS = 1ll << 22;    // slot publication wait (with nanosleep): ~1 s
 constexpr long long MBAR_SPINS = 1ll << 24;    // bulk-copy completion wait
 
 // MurmurHash3's 64-bit finaliser (Appleby, public domain).
@@ -402,7 +401,7 @@ __device__ void resolve(const LevelArgs &A, const Gen &g, u64 fp, bool active, u
         // Waits on other warps' publications (bounded).
         if (state == S_WAIT) {
             u32 f = FIELD_PENDING;
-            for (long long s = 0; s < WAIT_SPINS; ++s) {
+            for (long long s = 0; s < A.wait_spins; ++s) {
                 f = (u32)ld_acquire(A.slots + idx);
                 if (f != FIELD_PENDING) break;
                 __nanosleep(128);
@@ -1056,14 +1055,21 @@ cudaError_t launch_eval_formula(const int *prog, int len, const u64 *atoms, cons
 
 int level_kernel_smem_bytes(int left_tile, int pitch) { return left_tile * pitch * 8; }
 
+// The dynamic shared-memory limit is a per-device function attribute: each device keeps the
+// largest size enabled on it so far (0 = the 48 KiB default).
 template <int TL, int HK>
 static cudaError_t smem_attr(int smem) {
-    static std::atomic<int> attr_set{48 * 1024};  // largest dynamic shared memory size enabled so far
-    if (smem <= attr_set.load()) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(level_kernel<TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess) {
-        int cur = attr_set.load();
-        while (cur < smem && !attr_set.compare_exchange_weak(cur, smem)) {
+    constexpr int MAX_DEVICES = 64;
+    static std::atomic<int> attr_set[MAX_DEVICES];
+    if (smem <= 48 * 1024) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < MAX_DEVICES && smem <= attr_set[dev].load()) return cudaSuccess;
+    e = cudaFuncSetAttribute(level_kernel<TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess && dev >= 0 && dev < MAX_DEVICES) {
+        int cur = attr_set[dev].load();
+        while (cur < smem && !attr_set[dev].compare_exchange_weak(cur, smem)) {
         }
     }
     return e;

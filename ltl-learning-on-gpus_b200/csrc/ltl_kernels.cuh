@@ -126,6 +126,7 @@ struct LevelArgs {
     int right_chunk_big, unary_rows_big;
     int small_rows;      // small levels: right rows (unary: source-row pairs) per warp and item
     int hash_kind;       // fingerprint kind of the operator kernels (0 multiply-add, 1 fmix64)
+    long long wait_spins;   // polls (~128 ns apart) before a wait for a slot publication gives up
     long long small_level;  // levels with fewer candidates use one row per warp per item
     long long cap_rows;
     u64 *cache;

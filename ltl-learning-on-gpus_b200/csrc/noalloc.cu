@@ -32,6 +32,7 @@ constexpr int NOALLOC_MAX_TRACES = 64;
 constexpr int NOALLOC_SLOTS_LOG2 = 18;                 // 2^18 eight-byte slots = 2 MiB
 constexpr int NOALLOC_MAX_DEVICES = 64;
 constexpr int WALK_CAP = 1024;
+constexpr int NOALLOC_MIN_FORMULA = 16;                // holds "see_the_error", "not_found" and a letter
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
@@ -122,7 +123,8 @@ void write_node(const u64 *ent, int count, u64 parent, const char *alpha, int na
 
 extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_options *opt, char *formula,
                                            int32_t formula_cap, int32_t *cost_out, uint64_t *all_ltls_out) {
-    if (!t || !opt || !formula || formula_cap < 2 || !ltlg::traces_well_formed(t)) return LTLG_BAD_ARGS;
+    if (!t || !opt || !formula || formula_cap < NOALLOC_MIN_FORMULA || !ltlg::traces_well_formed(t))
+        return LTLG_BAD_ARGS;
     formula[0] = 0;
     const int *cf = opt->cost_fun;
     for (int i = 0; i < 8; ++i)
@@ -170,9 +172,15 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
         }
     }
     if (n == 0 || nalpha == 0) {
+        // nothing to enumerate: every level is empty (with no traces every letter separates
+        // them vacuously, and the first one is the answer at cost c1)
+        if (all_ltls_out) *all_ltls_out = all;
+        if (letter_hit >= 0) {
+            snprintf(formula, formula_cap, "%c", t->alphabet[letter_hit]);
+            return LTLG_FOUND;
+        }
         snprintf(formula, formula_cap, "not_found");
         if (cost_out) *cost_out = opt->max_cost > c1 ? opt->max_cost : c1;
-        if (all_ltls_out) *all_ltls_out = all;
         return LTLG_NOT_FOUND;
     }
 
@@ -263,6 +271,7 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     A.unary_rows_big = 64;
     A.small_rows = 1;
     A.small_level = max_grid * 2048ll;
+    A.wait_spins = 1ll << 22;
     A.hash_kind = hk;
     A.cap_rows = cap;
     A.cache = cache;
@@ -290,6 +299,7 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
             return LTLG_CUDA_ERROR;
         if (hc.status & (ST_WAIT | ST_TMA)) return LTLG_DEVICE_WAIT;
         if (hc.status & ST_TABLE) return LTLG_TABLE_FULL;
+        if (head[1] == 2) return LTLG_BAD_ARGS;  // more splits in a level than one plan holds
         if (head[1] == 0) last_cost = head[0];
         if (hc.found && opt->stop_at_found) break;
         if (hc.status & ST_OVERFLOW) return LTLG_NO_MEMORY;
@@ -342,12 +352,18 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     u64 ent[2 + 2 * WALK_CAP];
     if ((err = cudaMemcpy(ent, walk, sizeof(ent), cudaMemcpyDeviceToHost)) != cudaSuccess) return LTLG_CUDA_ERROR;
     const u64 count = ent[0], overflow = ent[1];
-    if (overflow || count - 1 >= 200) {
-        snprintf(formula, formula_cap, "Size of the output is too big");
+    if (overflow || count - 1 >= 200) {  // the reference's sentinel for more than 199 nodes
+        static const char big[] = "Size of the output is too big";
+        if ((int)sizeof(big) > formula_cap) return LTLG_FORMULA_TOO_LONG;
+        memcpy(formula, big, sizeof(big));
         return LTLG_FOUND;
     }
     Writer w{formula, formula_cap, 0, false};
     formula[0] = 0;
     write_node(ent + 2, (int)count, p, t->alphabet, nalpha, w, 0);
-    return w.over ? LTLG_BAD_ARGS : LTLG_FOUND;
+    if (w.over) {  // the search succeeded; only the caller's buffer is too small
+        formula[0] = 0;
+        return LTLG_FORMULA_TOO_LONG;
+    }
+    return LTLG_FOUND;
 }

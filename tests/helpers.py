@@ -57,3 +57,32 @@ def on_the_fly_cases(inst, costs, max_cost=14):
     return ex, [(k, ex.level_start[k + 1]) for k in range(costs[0] + 1, ex.cost - 1)
                 if ex.level_start[k + 2] > ex.level_start[k + 1] > len(inst.alphabet)]
 
+
+
+def edge_instance(pos_steps, neg_steps, alphabet="pq"):
+    """An instance from explicit step masks (lists of lists of ints), empty traces allowed."""
+    from ltlb200 import gen
+    traces = list(pos_steps) + list(neg_steps)
+    offs = np.zeros(len(traces) + 1, dtype=np.int32)
+    for i, t in enumerate(traces):
+        offs[i + 1] = offs[i] + len(t)
+    steps = np.array([m for t in traces for m in t], dtype=np.uint32)
+    return gen.Instance(len(pos_steps), len(neg_steps), alphabet, steps, offs)
+
+
+P_BIT, Q_BIT = 1 << (ord("p") - 97), 1 << (ord("q") - 97)
+
+
+def edge_cases():
+    """Inputs at the domain's edges: an empty side, a trace of no steps, one-step traces, a
+    trace of the maximum 63 steps, duplicate traces, and one trace on both sides."""
+    P, Q = P_BIT, Q_BIT
+    return {
+        "no_negatives": edge_instance([[P, Q], [P | Q]], []),
+        "no_positives": edge_instance([], [[P], [Q, 0, P]]),
+        "empty_trace": edge_instance([[P, 0, Q]], [[], [Q]]),
+        "one_step_traces": edge_instance([[P], [P | Q]], [[Q], [0]]),
+        "max_length_trace": edge_instance([[P if k % 3 else Q for k in range(63)]], [[Q] * 63, [P] * 5]),
+        "duplicate_traces": edge_instance([[P, Q], [P, Q]], [[Q, P], [Q, P]]),
+        "contradiction": edge_instance([[P, Q]], [[P, Q]]),
+    }

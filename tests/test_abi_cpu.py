@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     lib = api.lib()
-    assert lib.ltlg_abi_version() == 1
+    assert lib.ltlg_abi_version() == api.ABI_VERSION
     assert api.status_string(api.NOT_FOUND) == "not_found"
     assert api.status_string(api.INPUT_LIMITS) == "see_the_error"
 
@@ -195,12 +195,43 @@ def test_header_is_plain_c(tmp_path):
     src = tmp_path / "c_abi.c"
     src.write_text('#include "ltlgpu.h"\n'
                    "int main(void) { ltlg_options o; ltlg_default_options(&o);\n"
-                   "  return (o.max_cost == 500 && ltlg_abi_version() == 1) ? 0 : 1; }\n")
+                   "  return (o.max_cost == 500 && ltlg_abi_version() == LTLG_ABI_VERSION) ? 0 : 1; }\n")
     lib_dir = os.path.dirname(api.LIB_PATH)
     exe = tmp_path / "c_abi"
     subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
                     str(src), "-L", lib_dir, "-lltlgpu", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
     assert subprocess.run([str(exe)]).returncode == 0
+
+
+def test_struct_layouts_match_ctypes(tmp_path):
+    """Sizes and field offsets of the ABI structs as a C compiler lays them out equal the ctypes
+    mirrors the Python binding passes across the boundary."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    checks = {"ltlg_engine_config": (api.EngineConfig, ["slots_log2", "cache_bytes", "small_rows", "wait_spins",
+                                                        "small_level"]),
+              "ltlg_options": (api.Options, ["max_cost", "stop_at_found", "time_limit_s"]),
+              "ltlg_result": (api.Result, ["formula", "levels", "blocks", "launches"]),
+              "ltlg_traces": (api.Traces, ["alphabet", "steps", "offsets"]),
+              "ltlg_block_record": (api.BlockRecord, ["candidates", "features"])}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ltlgpu.h"', "int main(void) {"]
+    for cname, (_, fields) in checks.items():
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        for f in fields:
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {f}));')
+    lines.append("  return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = []
+    for _, (cls, fields) in checks.items():
+        want.append(ctypes.sizeof(cls))
+        want.extend(getattr(cls, f).offset for f in fields)
+    assert got == want
 
 
 def test_null_handles_and_no_device():

@@ -9,7 +9,7 @@ import pytest
 
 import oracle as O
 from ltlb200 import gen
-from helpers import last_round_gap, load_fixture, on_the_fly_cases, row_set
+from helpers import edge_cases, last_round_gap, load_fixture, on_the_fly_cases, row_set
 
 OPS = ["~", "&", "|", "X", "F", "G", "U"]
 
@@ -223,26 +223,7 @@ def test_oracle_on_the_fly_regime(costs):
     assert found >= 1
 
 
-def _edge(pos_steps, neg_steps, alphabet="pq"):
-    """An instance from explicit step masks (lists of lists of ints), empty traces allowed."""
-    traces = list(pos_steps) + list(neg_steps)
-    offs = np.zeros(len(traces) + 1, dtype=np.int32)
-    for i, t in enumerate(traces):
-        offs[i + 1] = offs[i] + len(t)
-    steps = np.array([m for t in traces for m in t], dtype=np.uint32)
-    return gen.Instance(len(pos_steps), len(neg_steps), alphabet, steps, offs)
-
-
-P, Q = 1 << (ord("p") - 97), 1 << (ord("q") - 97)
-EDGE = {
-    "no_negatives": _edge([[P, Q], [P | Q]], []),
-    "no_positives": _edge([], [[P], [Q, 0, P]]),
-    "empty_trace": _edge([[P, 0, Q]], [[], [Q]]),
-    "one_step_traces": _edge([[P], [P | Q]], [[Q], [0]]),
-    "max_length_trace": _edge([[P if k % 3 else Q for k in range(63)]], [[Q] * 63, [P] * 5]),
-    "duplicate_traces": _edge([[P, Q], [P, Q]], [[Q, P], [Q, P]]),
-    "contradiction": _edge([[P, Q]], [[P, Q]]),
-}
+EDGE = edge_cases()
 
 
 @pytest.mark.parametrize("name", sorted(EDGE))

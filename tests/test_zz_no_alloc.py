@@ -16,12 +16,12 @@ import pytest
 
 import oracle as O
 from ltlb200 import api, gen
-from helpers import load_fixture
+from helpers import edge_instance, load_fixture
 
 pytestmark = pytest.mark.gpu
 
 
-def noalloc(inst, **kw):
+def noalloc(inst, cap=api.FORMULA_MAX_BYTES, **kw):
     L = api.lib()
     f = L.ltlg_learn_noalloc
     f.argtypes = [C.POINTER(api.Traces), C.POINTER(api.Options), C.c_char_p, C.c_int32, C.POINTER(C.c_int32),
@@ -29,9 +29,9 @@ def noalloc(inst, **kw):
     f.restype = C.c_int
     t, keep = api._traces(inst)
     o = api.make_options(**kw)
-    buf = C.create_string_buffer(4096)
+    buf = C.create_string_buffer(cap)
     cost, all_ltls = C.c_int32(), C.c_uint64()
-    rc = f(C.byref(t), C.byref(o), buf, 4096, C.byref(cost), C.byref(all_ltls))
+    rc = f(C.byref(t), C.byref(o), buf, cap, C.byref(cost), C.byref(all_ltls))
     return rc, buf.value.decode(), cost.value, all_ltls.value
 
 
@@ -68,3 +68,45 @@ def test_noalloc_rejects_more_than_64_traces():
     inst = load_fixture("over64.trace")
     rc, formula, _, _ = noalloc(inst)
     assert rc == api.INPUT_LIMITS and formula == "see_the_error"
+
+
+def test_noalloc_no_traces_follows_learn():
+    """With no traces every letter separates them (vacuously): both entry points answer with
+    the first letter at the letter cost, whether or not the search stops at the find."""
+    inst = edge_instance([], [])
+    for stop in (True, False):
+        want = api.learn(inst, neg_type=1, max_cost=4, stop_at_found=stop)
+        for _ in range(2):
+            rc, formula, cost, all_ltls = noalloc(inst, neg_type=1, max_cost=4, stop_at_found=stop)
+            assert (rc, formula, cost, all_ltls) == (want.status, want.formula, want.cost, want.all_ltls)
+
+
+def test_noalloc_rejects_long_traces():
+    inst = load_fixture("len64.trace")
+    want = api.learn(inst)
+    rc, formula, _, _ = noalloc(inst)
+    assert rc == want.status == api.INPUT_LIMITS and formula == "see_the_error"
+
+
+def test_noalloc_scratch_overflow_is_reported():
+    """Levels beyond what the static scratch holds (about 131k rows of 40 traces) end the call
+    with LTLG_NO_MEMORY, on every call; the next call that fits is right again."""
+    inst = load_fixture("cfg1_deep.trace")
+    for _ in range(2):
+        rc, formula, _, _ = noalloc(inst, neg_type=1, max_cost=10, stop_at_found=False)
+        assert rc == api.NO_MEMORY
+    small = gen.generate(3, 2, 20, 20, 8, 16, 0.5, 5)
+    rc, formula, cost, _ = noalloc(small, neg_type=1)
+    assert rc == api.FOUND and cost == api.learn(small, neg_type=1).cost and O.separates(formula, small)
+
+
+def test_noalloc_formula_longer_than_buffer():
+    """A found formula that does not fit the caller's buffer is its own status, not a bad
+    argument: the string is empty, the cost and the candidate count are set."""
+    inst = load_fixture("cfg1_deep.trace")
+    want = api.learn(inst, neg_type=1)
+    assert want.status == api.FOUND and len(want.formula) >= 16
+    rc, formula, cost, all_ltls = noalloc(inst, cap=16, neg_type=1)
+    assert rc == api.FORMULA_TOO_LONG and formula == "" and cost == want.cost and all_ltls > 0
+    rc, formula, cost, _ = noalloc(inst, neg_type=1)
+    assert rc == api.FOUND and cost == want.cost and O.separates(formula, inst)

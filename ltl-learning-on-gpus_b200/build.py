@@ -17,7 +17,7 @@ CUFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisib
 LIB = os.path.join(OUT, "libltlgpu.so")
 CLI = os.path.join(OUT, "ltli6463")
 
-LIB_SOURCES = ["ltl_kernels.cu", "plan.cu", "engine.cu", "scarlet.cpp", "noalloc.cu", "mlp.cu", "evaluate.cu"]
+LIB_SOURCES = ["learn.cu", "engine.cu", "scarlet.cpp", "noalloc.cu", "mlp.cu", "evaluate.cu"]
 
 
 def _newer(target, deps):

@@ -2,22 +2,23 @@
 //
 // ltlg_engine_learn restates LTLI (code/ltli6463.cu:1043-1497) for the GPU path:
 //   letters and the early letter hit ........ :1058-1136
-//   level / operator / split order ........... :1199-1445 (NegType rule :1212)
+//   level / operator / split order ........... :1199-1445 (NegType rule :1212), planned on the device
+//   the find and the candidate count ......... :1232-1234 (first block in order that holds one)
 //   on-the-fly overflow regime ............... :1021-1027, :1202-1206, :1442-1443
 //   found -> formula string, 200-node limit .. :877-991
-// The per-chunk host round trips of the reference are gone: a level is one launch
-// (or one launch per block in the per-block schedule), and the host reads a small
-// control record once per level.
+// The reference's per-chunk host round trips are gone: a learn is one persistent launch of the
+// level kernel, which plans every next level on the device.  The per-block schedule (the
+// reference's progress lines) and the on-the-fly regime run level by level from the host.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
-#include <thread>
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ltl_kernels.cuh"
@@ -58,8 +59,6 @@ double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-const char OPCH[7] = {'~', '&', '|', 'X', 'F', 'G', 'U'};
-
 u64 host_fmix64(u64 x) {
     x ^= x >> 33;
     x *= 0xff51afd7ed558ccdull;
@@ -82,33 +81,33 @@ u64 host_fingerprint_exact(const uint64_t *w, int n, int pitch) {
     return host_fmix64(sum);
 }
 
+// Entries per level plan: 4 unary blocks and, per binary operator, a split per cost up to
+// max_cost / 2.
+long long entries_for(int max_cost) { return 4 + 3 * ((long long)max_cost / 2 + 2); }
+
 }  // namespace
 
 struct ltlg_engine {
     ltlg_engine_config cfg{};
     int num_sms = 0;
     cudaStream_t stream = nullptr;
-    static constexpr int RING = 4;     // levels in flight: the host runs up to RING - 1 ahead
-    cudaEvent_t ev_start[RING] = {}, ev_done[RING] = {};
-    cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
-    DevBuf cache, parents, keys, slots, wmeta, kmeta, ctl, walk, snaps, lev, ls, lcands, args;
-    // One graph per ring slot: planner, level kernel, and the copy of the level's control
-    // block and plan header into that slot.  The kernels read their
-    // arguments from `args`, so the graphs stay valid from one learn to the next; they are
-    // captured again only when the kernel instances or grids change (graph_key).
-    cudaGraphExec_t level_graph[RING] = {};
-    void *ring_dev = nullptr;       // device view of h_ring
-    DevBuf scorer, scorer_params;   // the learned block order's scorer (MlpDev, packed FP32)
-    DevBuf lstats, h_lstats;        // row statistics per cost (LSTATS counters)
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    // device buffers of the instance
+    DevBuf cache, parents, keys, slots, wmeta, kmeta, ls, ne, lcands, lns, lstats, entries, fpar;
+    DevBuf ctl, args, launch, walk, snaps, scorer, scorer_params;
+    // pinned host copies
+    DevBuf h_ctl, h_args, h_launch, h_walk, h_stage, h_ls, h_lcands, h_lns, h_ne, h_snaps, h_win, h_entries, h_fpar,
+        h_lstats;
+    volatile u32 *cancel = nullptr;  // mapped host flag read by the planner
+    void *cancel_dev = nullptr;
     bool has_scorer = false;
-    long long graph_key[8] = {};
-    DevBuf h_ctl, h_walk, h_stage, h_snaps, h_args, h_lev, h_ls, h_lcands, h_win, h_ring;
-
     u64 nslots = 0;
     u32 gen = 0;
     // last learn
-    int n = 0, pitch = 0, nalpha = 0;
+    int n = 0, pitch = 0, nalpha = 0, max_cost = 0;
     long long cap_rows = 0;
+    int tile = 0, stages = 0, grid = 0, hk = 0;
+    long long tile_bytes = 0;
     std::vector<long long> level_start;
     std::string last_error;
 };
@@ -125,17 +124,24 @@ int fail_cuda(ltlg_engine *e, cudaError_t err, ltlg_result *res) {
     return LTLG_CUDA_ERROR;
 }
 
+int fail_status(ltlg_result *res, int status) {
+    res->status = status;
+    free(res->formula);
+    res->formula = strdup(ltlg_status_string(status));
+    return status;
+}
+
 struct Block {
     int op, lcost, rcost;
     long long l0, l1, r0, r1;
     long long candidates;  // as the reference counts them (U: 2 per pair)
 };
 
-// Blocks of cost c in the reference's order (ltli6463.cu:1209-1440).
+// Blocks of cost c in the reference's order (ltli6463.cu:1209-1440); positions are indices.
 std::vector<Block> level_blocks(int c, const int *cf, int neg_type, const std::vector<long long> &ls) {
     const int c1 = cf[0];
-    auto lo = [&](int k) { return (k >= 0 && k + 1 < (int)ls.size()) ? ls[k] : 0ll; };
-    auto hi = [&](int k) { return (k >= 0 && k + 1 < (int)ls.size()) ? ls[k + 1] : 0ll; };
+    auto lo = [&](int k) { return (k >= c1 && k < c && k + 1 < (int)ls.size()) ? ls[k] : 0ll; };
+    auto hi = [&](int k) { return (k >= c1 && k < c && k + 1 < (int)ls.size()) ? ls[k + 1] : 0ll; };
     std::vector<Block> out;
     auto unary = [&](int op, int k) {
         const long long a = lo(k), b = hi(k);
@@ -156,28 +162,6 @@ std::vector<Block> level_blocks(int c, const int *cf, int neg_type, const std::v
     if (c - cf[6] >= c1) unary(OP_G, c - cf[6]);
     binary(OP_U, cf[7]);
     return out;
-}
-
-// The window of block (op, k) in a host copy of a plan: items [lo, hi) of the level's item
-// table (unary blocks must be unfused, one per operator).
-void block_window(const DevLevel *hl, int op, int k, long long &lo, long long &hi) {
-    const bool un = op == OP_NEG || op == OP_X || op == OP_F || op == OP_G;
-    for (int r = 0; r < hl->nranges; ++r) {
-        const ItemRange &R = hl->ranges[r];
-        if (un ? (R.cls == 1 && hl->ublocks[R.idx].op == op) : (R.cls != 1 && R.idx == op * MAX_SPLITS + k)) {
-            lo = R.item0;
-            hi = r + 1 < hl->nranges ? hl->ranges[r + 1].item0 : hl->items_end;
-            return;
-        }
-    }
-    lo = hi = 0;
-}
-
-int cost_of_row(const std::vector<long long> &ls, long long row) {
-    // ls[k] .. ls[k + 1] are the rows of cost k
-    for (int k = (int)ls.size() - 2; k >= 0; --k)
-        if (row >= ls[k] && row < ls[k + 1]) return k;
-    return -1;
 }
 
 void build_string(const std::map<u64, u64> &par, u64 row, u64 p, bool is_root, const std::string &alpha, int nalpha,
@@ -214,6 +198,28 @@ void build_string(const std::map<u64, u64> &par, u64 row, u64 p, bool is_root, c
     }
 }
 
+// Level-kernel geometry for rows of `pitch` words: the left tile (shrunk from `want` until at
+// least three item slots fit the shared memory) and the slots.  Returns false when not even one
+// slot of a 2-row tile fits.
+bool geometry(int want, int pitch, int &tile, int &stages, long long &tile_bytes) {
+    constexpr long long BUDGET = 200 * 1024;  // dynamic shared memory for the slots' tiles
+    tile = want;
+    while (tile > 2 && BUDGET / ((long long)tile * pitch * 8) < 3) tile /= 2;
+    tile_bytes = (long long)tile * pitch * 8;
+    stages = (int)std::min<long long>(8, BUDGET / tile_bytes);
+    return stages >= 1;
+}
+
+// What the level loop of one learn ends with.
+struct LoopOut {
+    int status = LTLG_NOT_FOUND;
+    bool found = false, on_the_fly = false;
+    int last_cost = 0;
+    double device_ms = 0;
+    int launches = 0;
+    std::vector<ltlg_block_stat> bstats;
+};
+
 }  // namespace
 
 extern "C" {
@@ -244,7 +250,7 @@ LTLG_API void ltlg_default_engine_config(ltlg_engine_config *c) {
     c->cache_bytes = 16ll << 30;
     c->max_rows = 64ll << 20;
     c->max_traces = 8192;
-    c->block_threads = 256;
+    c->block_threads = LEVEL_THREADS;
     c->left_tile = 4;
     c->right_chunk = 16;
     c->unary_rows = 32;
@@ -277,7 +283,6 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
     if (cfg.device < 0 || cfg.device >= ndev) return LTLG_BAD_ARGS;
     if (cfg.slots_log2 < 10 || cfg.slots_log2 > 34) return LTLG_BAD_ARGS;
     if (cfg.left_tile != 2 && cfg.left_tile != 4 && cfg.left_tile != 8) return LTLG_BAD_ARGS;
-    if (cfg.block_threads < 32 || cfg.block_threads > 256 || cfg.block_threads % 32) return LTLG_BAD_ARGS;
     if (cfg.right_chunk < 1 || cfg.unary_rows < 1 || cfg.max_traces < 1 || cfg.wait_spins < 0 ||
         cfg.small_level < 0)
         return LTLG_BAD_ARGS;
@@ -287,44 +292,29 @@ LTLG_API int ltlg_engine_create(const ltlg_engine_config *cfg_in, ltlg_engine **
     cudaError_t err = cudaSetDevice(cfg.device);
     if (err == cudaSuccess) err = cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, cfg.device);
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
-    for (int k = 0; k < ltlg_engine::RING && err == cudaSuccess; ++k) {
-        err = cudaEventCreate(&e->ev_start[k]);
-        if (err == cudaSuccess) err = cudaEventCreate(&e->ev_done[k]);
-    }
     if (err == cudaSuccess) err = cudaEventCreate(&e->ev_a);
     if (err == cudaSuccess) err = cudaEventCreate(&e->ev_b);
-    if (err == cudaSuccess) err = cudaEventCreate(&e->ev_t0);
-    if (err == cudaSuccess) err = cudaEventCreate(&e->ev_t1);
     e->nslots = 1ull << cfg.slots_log2;
     if (err == cudaSuccess) err = ensure(e->slots, e->nslots * 8);
     if (err == cudaSuccess) err = cudaMemsetAsync(e->slots.p, 0, e->nslots * 8, e->stream);
     if (err == cudaSuccess) err = ensure(e->cache, (size_t)cfg.cache_bytes);
-    if (err == cudaSuccess) err = ensure(e->ctl, sizeof(DevCtl));
-    if (err == cudaSuccess) err = ensure_host(e->h_ctl, sizeof(DevCtl));
+    if (err == cudaSuccess) err = ensure(e->ctl, sizeof(InstCtl));
+    if (err == cudaSuccess) err = ensure_host(e->h_ctl, sizeof(InstCtl));
+    if (err == cudaSuccess) err = ensure(e->args, sizeof(InstArgs));
+    if (err == cudaSuccess) err = ensure_host(e->h_args, sizeof(InstArgs));
+    if (err == cudaSuccess) err = ensure(e->launch, sizeof(Launch));
+    if (err == cudaSuccess) err = ensure_host(e->h_launch, sizeof(Launch));
     if (err == cudaSuccess) err = ensure(e->walk, (2 + 2 * 1024) * 8);
     if (err == cudaSuccess) err = ensure_host(e->h_walk, (2 + 2 * 1024) * 8);
-    const size_t max_blocks = 7 * MAX_SPLITS;
-    if (err == cudaSuccess) err = ensure(e->snaps, max_blocks * sizeof(DevCtl));
-    if (err == cudaSuccess) err = ensure_host(e->h_snaps, max_blocks * sizeof(DevCtl));
-    if (err == cudaSuccess) err = ensure_host(e->h_win, max_blocks * 8 * sizeof(long long));
-    if (err == cudaSuccess) err = ensure_host(e->h_args, sizeof(LevelArgs));
-    if (err == cudaSuccess) err = ensure(e->args, sizeof(LevelArgs));
-    if (err == cudaSuccess) err = ensure(e->lstats, (MAX_COSTS + 2) * LSTATS * sizeof(u64));
-    if (err == cudaSuccess) err = ensure_host(e->h_lstats, (MAX_COSTS + 2) * LSTATS * sizeof(u64));
-    if (err == cudaSuccess) {  // the ring of level summaries: mapped, the level kernel writes it
-        err = cudaHostAlloc(&e->h_ring.p, ltlg_engine::RING * (sizeof(DevCtl) + sizeof(DevLevel)), cudaHostAllocMapped);
+    if (err == cudaSuccess) {
+        void *p = nullptr;
+        err = cudaHostAlloc(&p, 64, cudaHostAllocMapped);
         if (err == cudaSuccess) {
-            e->h_ring.bytes = ltlg_engine::RING * (sizeof(DevCtl) + sizeof(DevLevel));
-            memset(e->h_ring.p, 0, e->h_ring.bytes);
-            err = cudaHostGetDevicePointer(&e->ring_dev, e->h_ring.p, 0);
+            memset(p, 0, 64);
+            e->cancel = (volatile u32 *)p;
+            err = cudaHostGetDevicePointer(&e->cancel_dev, p, 0);
         }
     }
-    if (err == cudaSuccess) err = ensure(e->lev, sizeof(DevLevel));
-    if (err == cudaSuccess) err = ensure_host(e->h_lev, sizeof(DevLevel));
-    if (err == cudaSuccess) err = ensure(e->ls, (MAX_COSTS + 2) * sizeof(long long));
-    if (err == cudaSuccess) err = ensure_host(e->h_ls, (MAX_COSTS + 2) * sizeof(long long));
-    if (err == cudaSuccess) err = ensure(e->lcands, (MAX_COSTS + 2) * sizeof(u64));
-    if (err == cudaSuccess) err = ensure_host(e->h_lcands, (MAX_COSTS + 2) * sizeof(u64));
     if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
     if (err != cudaSuccess) {
         ltlg_engine_destroy(e);
@@ -338,19 +328,16 @@ LTLG_API void ltlg_engine_destroy(ltlg_engine *e) {
     if (!e) return;
     cudaSetDevice(e->cfg.device);
     if (e->stream) cudaStreamSynchronize(e->stream);
-    for (cudaGraphExec_t g : e->level_graph)
-        if (g) cudaGraphExecDestroy(g);
-    for (DevBuf *b : {&e->cache, &e->parents, &e->keys, &e->slots, &e->wmeta, &e->kmeta, &e->ctl, &e->walk, &e->snaps,
-                      &e->lev, &e->ls, &e->lcands, &e->args, &e->scorer, &e->scorer_params, &e->lstats})
+    for (DevBuf *b : {&e->cache, &e->parents, &e->keys, &e->slots, &e->wmeta, &e->kmeta, &e->ls, &e->ne, &e->lcands,
+                      &e->lns, &e->lstats, &e->entries, &e->fpar, &e->ctl, &e->args, &e->launch, &e->walk, &e->snaps,
+                      &e->scorer, &e->scorer_params})
         if (b->p) cudaFree(b->p);
-    for (DevBuf *b : {&e->h_ctl, &e->h_walk, &e->h_stage, &e->h_snaps, &e->h_args, &e->h_lev, &e->h_ls, &e->h_lcands,
-                      &e->h_win, &e->h_ring, &e->h_lstats})
+    for (DevBuf *b : {&e->h_ctl, &e->h_args, &e->h_launch, &e->h_walk, &e->h_stage, &e->h_ls, &e->h_lcands, &e->h_lns,
+                      &e->h_ne, &e->h_snaps, &e->h_win, &e->h_entries, &e->h_fpar, &e->h_lstats})
         if (b->p) cudaFreeHost(b->p);
-    for (cudaEvent_t ev : {e->ev_a, e->ev_b, e->ev_t0, e->ev_t1})
+    if (e->cancel) cudaFreeHost((void *)e->cancel);
+    for (cudaEvent_t ev : {e->ev_a, e->ev_b})
         if (ev) cudaEventDestroy(ev);
-    for (int k = 0; k < ltlg_engine::RING; ++k)
-        for (cudaEvent_t ev : {e->ev_start[k], e->ev_done[k]})
-            if (ev) cudaEventDestroy(ev);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -363,34 +350,83 @@ LTLG_API void ltlg_result_free(ltlg_result *r) {
     memset(r, 0, sizeof(*r));
 }
 
+}  // extern "C"
+
+namespace {
+
+// Runs the level kernel once over the engine's instance and waits for it, with the learn's
+// time limit (the planner ends the search at the next level boundary once the cancel flag is set).
+cudaError_t run_levels(ltlg_engine *e, bool persist, int grid, double t0, double time_limit_s, LoopOut &o) {
+    Launch *hl = (Launch *)e->h_launch.p;
+    hl->args = (const InstArgs *)e->args.p;
+    hl->ninst = 1;
+    hl->persist = persist ? 1 : 0;
+    hl->tile = e->tile;
+    hl->stages = e->stages;
+    hl->tile_bytes = e->tile_bytes;
+    cudaStream_t st = e->stream;
+    cudaError_t err = cudaMemcpyAsync(e->launch.p, hl, sizeof(Launch), cudaMemcpyHostToDevice, st);
+    if (err != cudaSuccess) return err;
+    cudaEventRecord(e->ev_a, st);
+    err = launch_levels(*hl, (const Launch *)e->launch.p, grid, e->hk, st);
+    if (err != cudaSuccess) return err;
+    cudaEventRecord(e->ev_b, st);
+    ++o.launches;
+    if (time_limit_s > 0) {
+        while ((err = cudaEventQuery(e->ev_b)) == cudaErrorNotReady) {
+            if (now_s() - t0 > time_limit_s) *e->cancel = 1u;
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+        if (err != cudaSuccess) return err;
+    } else if ((err = cudaEventSynchronize(e->ev_b)) != cudaSuccess) {
+        return err;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev_a, e->ev_b);
+    o.device_ms += ms;
+    return cudaSuccess;
+}
+
+cudaError_t read_ctl(ltlg_engine *e, InstCtl *hc) {
+    cudaError_t err = cudaMemcpyAsync(hc, e->ctl.p, sizeof(InstCtl), cudaMemcpyDeviceToHost, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    return err;
+}
+
+// Opens items [lo, hi) of the current plan (sequence seq) for claiming.
+cudaError_t open_window(ltlg_engine *e, u32 seq, long long lo, long long hi, int slot) {
+    u64 *w = (u64 *)e->h_win.p + 2 * slot;
+    w[0] = ((u64)seq << SEQ_SHIFT) | (u64)lo;
+    w[1] = ((u64)seq << SEQ_SHIFT) | (u64)hi;
+    InstCtl *dc = (InstCtl *)e->ctl.p;
+    cudaError_t err = cudaMemcpyAsync(&dc->limit, &w[1], 8, cudaMemcpyHostToDevice, e->stream);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&dc->claimed, &w[0], 8, cudaMemcpyHostToDevice, e->stream);
+    return err;
+}
+
+int fatal_status(u32 f) { return (f & ST_TABLE) ? LTLG_TABLE_FULL : LTLG_DEVICE_WAIT; }
+
+}  // namespace
+
+extern "C" {
+
 LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_options *opt, ltlg_result *res) {
     memset(res, 0, sizeof(*res));
     const double t0 = now_s();
-    if (!e || !t || !opt) {
-        res->status = LTLG_BAD_ARGS;
-        res->formula = strdup("bad_arguments");
-        return res->status;
-    }
+    if (!e || !t || !opt) return fail_status(res, LTLG_BAD_ARGS);
     const int *cf = opt->cost_fun;
     for (int i = 0; i < 8; ++i)
-        if (cf[i] <= 0 || cf[i] > SHRT_MAX) {
-            res->status = LTLG_BAD_ARGS;
-            res->formula = strdup("bad_arguments");
-            return res->status;
-        }
+        if (cf[i] <= 0 || cf[i] > SHRT_MAX) return fail_status(res, LTLG_BAD_ARGS);
     const int c1 = cf[0];
     const int npos = t->num_pos, nneg = t->num_neg, n = npos + nneg;
     const std::string alpha = t->alphabet ? t->alphabet : "";
     const int nalpha = (int)alpha.size();
     const bool ref_keys = opt->key_mode == LTLG_KEY_REF;
     if (!traces_well_formed(t) || (ref_keys && (opt->rlx_unq_chk_type < 1 || opt->rlx_unq_chk_type > 3)) ||
-        opt->key_mode < 0 || opt->key_mode > 2 || n > e->cfg.max_traces || nalpha > 26 ||
-        (opt->order != LTLG_ORDER_PLAIN && opt->order != LTLG_ORDER_LEARNED) ||
-        (opt->order == LTLG_ORDER_LEARNED && !e->has_scorer)) {
-        res->status = LTLG_BAD_ARGS;
-        res->formula = strdup("bad_arguments");
-        return res->status;
-    }
+        opt->key_mode < 0 || opt->key_mode > 2 || n > e->cfg.max_traces || nalpha > 26 || opt->max_cost < 1 ||
+        opt->max_cost > SHRT_MAX || (opt->order != LTLG_ORDER_PLAIN && opt->order != LTLG_ORDER_LEARNED) ||
+        (opt->order == LTLG_ORDER_LEARNED && !e->has_scorer))
+        return fail_status(res, LTLG_BAD_ARGS);
     int max_len = 0, len_sum = 0;
     for (int i = 0; i < n; ++i) {
         const int ln = t->offsets[i + 1] - t->offsets[i];
@@ -428,13 +464,14 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
             if (opt->stop_at_found) break;
         }
     }
+    const int max_cost = opt->max_cost;
     e->n = n;
     e->pitch = pitch;
     e->nalpha = nalpha;
+    e->max_cost = max_cost;
     const long long cap_rows =
         std::min<long long>(e->cfg.max_rows, e->cfg.cache_bytes / ((long long)pitch * 8ll));
     e->cap_rows = cap_rows;
-    const int max_cost = opt->max_cost;
     e->level_start.assign((size_t)std::max(max_cost, c1) + 3, 0);
     for (size_t k = (size_t)c1 + 1; k < e->level_start.size(); ++k) e->level_start[k] = nalpha;
     if (letter_hit >= 0 && opt->stop_at_found) {
@@ -457,11 +494,19 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         res->seconds = now_s() - t0;
         return res->status;
     }
-    if (cap_rows < nalpha + 1) {
-        res->status = LTLG_NO_MEMORY;
-        res->formula = strdup("no_memory");
-        return res->status;
-    }
+    if (cap_rows < nalpha + 1) return fail_status(res, LTLG_NO_MEMORY);
+    int tile = 0, stages = 0;
+    long long tile_bytes = 0;
+    if (!geometry(e->cfg.left_tile, pitch, tile, stages, tile_bytes)) return fail_status(res, LTLG_BAD_ARGS);
+    const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
+    const size_t smem = level_kernel_smem(stages, tile_bytes);
+    const int per_sm = level_kernel_ctas_per_sm(hk, smem);
+    if (per_sm < 1) return fail_status(res, LTLG_BAD_ARGS);
+    e->tile = tile;
+    e->stages = stages;
+    e->tile_bytes = tile_bytes;
+    e->hk = hk;
+    e->grid = e->num_sms * per_sm;
 
     // Per-word metadata: length mask | positive flag; relaxed-key bit placement.
     std::vector<u64> wmeta(pitch, 0ull);
@@ -489,17 +534,34 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         }
     }
 
-    // Buffers
+    // Buffers (sized for this learn's max_cost: no cap on costs or splits)
+    const long long ncost = (long long)max_cost + 3;
+    const long long cap_entries = entries_for(max_cost);
+    const bool want_stats = opt->order == LTLG_ORDER_LEARNED || opt->record_levels >= 2;
     if ((err = ensure(e->parents, (size_t)cap_rows * 8)) != cudaSuccess) return fail_cuda(e, err, res);
     if (opt->key_mode != LTLG_KEY_EXACT && (err = ensure(e->keys, (size_t)cap_rows * 16)) != cudaSuccess)
         return fail_cuda(e, err, res);
     if ((err = ensure(e->wmeta, (size_t)pitch * 8)) != cudaSuccess) return fail_cuda(e, err, res);
     if ((err = ensure(e->kmeta, (size_t)pitch * 4)) != cudaSuccess) return fail_cuda(e, err, res);
+    if ((err = ensure(e->ls, (size_t)ncost * 8)) != cudaSuccess) return fail_cuda(e, err, res);
+    if ((err = ensure(e->ne, (size_t)ncost * 4)) != cudaSuccess) return fail_cuda(e, err, res);
+    if ((err = ensure(e->lcands, (size_t)ncost * 8)) != cudaSuccess) return fail_cuda(e, err, res);
+    if ((err = ensure(e->lns, (size_t)ncost * 8)) != cudaSuccess) return fail_cuda(e, err, res);
+    if ((err = ensure(e->lstats, (size_t)ncost * LSTATS * 8)) != cudaSuccess) return fail_cuda(e, err, res);
+    if ((err = ensure(e->entries, (size_t)(2 * cap_entries) * sizeof(Entry))) != cudaSuccess)
+        return fail_cuda(e, err, res);
+    if ((err = ensure(e->fpar, (size_t)cap_entries * 8)) != cudaSuccess) return fail_cuda(e, err, res);
+    if ((err = ensure(e->snaps, (size_t)cap_entries * 8)) != cudaSuccess) return fail_cuda(e, err, res);
     if ((err = ensure_host(e->h_stage, std::max<size_t>((size_t)nalpha * pitch * 8, (size_t)pitch * 12))) !=
-        cudaSuccess)
+            cudaSuccess ||
+        (err = ensure_host(e->h_ls, (size_t)ncost * 8)) != cudaSuccess ||
+        (err = ensure_host(e->h_lcands, (size_t)ncost * 8)) != cudaSuccess ||
+        (err = ensure_host(e->h_lns, (size_t)ncost * 8)) != cudaSuccess ||
+        (err = ensure_host(e->h_snaps, (size_t)cap_entries * 8)) != cudaSuccess ||
+        (err = ensure_host(e->h_win, (size_t)(2 * cap_entries + 2) * 8)) != cudaSuccess ||
+        (err = ensure_host(e->h_entries, (size_t)cap_entries * sizeof(Entry))) != cudaSuccess)
         return fail_cuda(e, err, res);
     cudaStream_t st = e->stream;
-    // staging: letters, then wmeta, then kmeta (synchronised before reuse)
     memcpy(e->h_stage.p, letters.data(), letters.size() * 8);
     if ((err = cudaMemcpyAsync(e->cache.p, e->h_stage.p, letters.size() * 8, cudaMemcpyHostToDevice, st)) !=
         cudaSuccess)
@@ -515,371 +577,253 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         cudaMemsetAsync(e->slots.p, 0, e->nslots * 8, st);
         e->gen = 1;
     }
-    DevCtl *hc = (DevCtl *)e->h_ctl.p;
-    memset(hc, 0, sizeof(DevCtl));
+    cudaMemsetAsync(e->ls.p, 0, (size_t)ncost * 8, st);
+    cudaMemsetAsync(e->lcands.p, 0, (size_t)ncost * 8, st);
+    cudaMemsetAsync(e->lns.p, 0, (size_t)ncost * 8, st);
+    if (want_stats) cudaMemsetAsync(e->lstats.p, 0, (size_t)ncost * LSTATS * 8, st);
+    InstCtl *hc = (InstCtl *)e->h_ctl.p;
+    memset(hc, 0, sizeof(InstCtl));
     hc->row_count = (u64)nalpha;
-    cudaMemcpyAsync(e->ctl.p, hc, sizeof(DevCtl), cudaMemcpyHostToDevice, st);
+    hc->found_key = NO_FIND;
+    hc->plan.cost = c1;
+    cudaMemcpyAsync(e->ctl.p, hc, sizeof(InstCtl), cudaMemcpyHostToDevice, st);
+    *e->cancel = 0u;
 
-    int tl = e->cfg.left_tile;
-    // shrink the left tile until three CTAs fit an SM's shared memory (long CS rows)
-    while (tl > 2 && 3 * (size_t)level_kernel_smem_bytes(tl, pitch) > 200 * 1024) tl /= 2;
-    if ((size_t)level_kernel_smem_bytes(tl, pitch) > 220 * 1024) {
-        res->status = LTLG_BAD_ARGS;
-        res->formula = strdup("bad_arguments");
-        return res->status;
-    }
-    const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
-    const int block_threads = e->cfg.block_threads;
-    // resident CTAs of the level kernel on all SMs
-    const long long max_grid =
-        (long long)e->num_sms * std::max(1, level_kernel_max_ctas_per_sm(tl, hk, block_threads, pitch));
-
-    // Arguments and plan in device memory.
-    DevLevel *dlev = (DevLevel *)e->lev.p;
-    LevelArgs *ha = (LevelArgs *)e->h_args.p;
-    memset(ha, 0, sizeof(LevelArgs));
-    LevelArgs &A = *ha;
+    const bool per_block = opt->schedule == LTLG_SCHEDULE_PER_BLOCK;
+    const bool learned = opt->order == LTLG_ORDER_LEARNED;
+    InstArgs *ha = (InstArgs *)e->h_args.p;
+    memset(ha, 0, sizeof(InstArgs));
+    InstArgs &A = *ha;
     A.n = n;
     A.pitch = pitch;
     A.npos = npos;
     A.nalpha = nalpha;
     A.key_mode = opt->key_mode == LTLG_KEY_EXACT ? KEY_EXACT : opt->key_mode == LTLG_KEY_REF ? KEY_REF : KEY_HASH64;
     A.rlx_type = rlx_type;
-    A.gen = e->gen;
     A.stop_at_found = opt->stop_at_found ? 1 : 0;
-    A.left_tile = tl;
+    A.find_first = learned ? 1 : 0;
     A.neg_type = opt->neg_type;
     A.max_cost = max_cost;
-    A.nwarps = block_threads / 32;
+    A.on_the_fly = 0;
+    A.plan_flags = (per_block ? PLAN_UNFUSED : 0) | (learned ? PLAN_LEARNED : 0);
     for (int i = 0; i < 8; ++i) A.cf[i] = cf[i];
     A.right_chunk_big = e->cfg.right_chunk;
     A.unary_rows_big = e->cfg.unary_rows;
-    A.small_level = e->cfg.small_level > 0 ? e->cfg.small_level : max_grid * 2048ll;
     A.small_rows = std::max(1, e->cfg.small_rows);
+    A.tile = tile;
+    A.gen = e->gen;
+    // small levels: where big items would give fewer than four per CTA
+    A.small_level = e->cfg.small_level > 0 ? e->cfg.small_level
+                                           : (long long)e->grid * 4 * tile * std::max(1, e->cfg.right_chunk);
     A.wait_spins = e->cfg.wait_spins > 0 ? e->cfg.wait_spins : (1ll << 22);
-    A.hash_kind = hk;
     A.cap_rows = cap_rows;
+    A.cap_entries = cap_entries;
+    A.learn_min_items = (long long)e->grid * stages;
+    A.slot_mask = e->nslots - 1;
     A.cache = (u64 *)e->cache.p;
     A.parents = (u64 *)e->parents.p;
     A.keys = opt->key_mode != LTLG_KEY_EXACT ? (u64 *)e->keys.p : nullptr;
     A.slots = (u64 *)e->slots.p;
-    A.slot_mask = e->nslots - 1;
     A.wmeta = (const u64 *)e->wmeta.p;
     A.kmeta = (const u32 *)e->kmeta.p;
-    A.ctl = (DevCtl *)e->ctl.p;
-    A.lev = dlev;
     A.ls = (long long *)e->ls.p;
+    A.ne = (int *)e->ne.p;
     A.level_cands = (u64 *)e->lcands.p;
-    A.model = opt->order == LTLG_ORDER_LEARNED ? e->scorer.p : nullptr;
-    A.grid = max_grid;
-    A.lstats = (u64 *)e->lstats.p;
-    A.ring = e->ring_dev;
-    A.ring_slots = ltlg_engine::RING;
-    cudaMemsetAsync(e->lstats.p, 0, (MAX_COSTS + 2) * LSTATS * sizeof(u64), st);
-    cudaMemsetAsync(e->ls.p, 0, (MAX_COSTS + 2) * sizeof(long long), st);
-    cudaMemsetAsync(e->lcands.p, 0, (MAX_COSTS + 2) * sizeof(u64), st);
-    DevLevel *hl = (DevLevel *)e->h_lev.p;
-    memset(hl, 0, offsetof(DevLevel, blocks));
-    hl->cost = c1;  // the planner advances to c1 + 1 first
-    hl->plan_flags = (opt->schedule == LTLG_SCHEDULE_PER_BLOCK ? PLAN_UNFUSED : 0) |
-                     (opt->order == LTLG_ORDER_LEARNED ? PLAN_LEARNED : 0);
-    cudaMemcpyAsync(dlev, hl, offsetof(DevLevel, blocks), cudaMemcpyHostToDevice, st);
-    const LevelArgs *dA = (const LevelArgs *)e->args.p;
-    cudaMemcpyAsync(e->args.p, ha, sizeof(LevelArgs), cudaMemcpyHostToDevice, st);
-    if ((err = launch_insert_letters(A, dA, nalpha, st)) != cudaSuccess) return fail_cuda(e, err, res);
-    int launches = 1;
+    A.level_ns = (u64 *)e->lns.p;
+    A.lstats = want_stats ? (u64 *)e->lstats.p : nullptr;
+    A.entries = (Entry *)e->entries.p;
+    A.found_par = (u64 *)e->fpar.p;
+    A.ctl = (InstCtl *)e->ctl.p;
+    A.model = learned ? e->scorer.p : nullptr;
+    A.cancel = (const volatile u32 *)e->cancel_dev;
+    const InstArgs *dA = (const InstArgs *)e->args.p;
+    cudaMemcpyAsync(e->args.p, ha, sizeof(InstArgs), cudaMemcpyHostToDevice, st);
+    if ((err = launch_insert_letters(dA, nalpha, hk, st)) != cudaSuccess) return fail_cuda(e, err, res);
+    const bool persist = !per_block;
+    if ((err = launch_first_plan(dA, 1, persist ? 1 : 0, st)) != cudaSuccess) return fail_cuda(e, err, res);
 
-    int status = LTLG_NOT_FOUND;
-    bool found = letter_hit >= 0, on_the_fly = false, last_round = false;
-    int shortage = -1, found_cost = found ? c1 : -1, last_cost = c1;
-    u64 found_word = 0;
-    u32 dflags = 0;
-    double device_ms = 0;
-    std::vector<ltlg_block_stat> bstats;
-    const bool per_block = opt->schedule == LTLG_SCHEDULE_PER_BLOCK;
-    const u32 fatal = ST_WAIT | ST_TMA | ST_TABLE;
-    auto fatal_status = [&](u32 f) { return (f & ST_TABLE) ? LTLG_TABLE_FULL : LTLG_DEVICE_WAIT; };
-
-    // ---- device-planned levels: per level one graph launch (the planner builds the plan from
-    // the level starts in device memory, then the level kernel runs it and its last CTA writes
-    // the level summary into the mapped host ring), enqueued up to RING - 1 levels ahead of
-    // the level the host is reading, so the GPU never waits for the host between levels.
-    bool host_mode = per_block;
-    std::vector<float> level_ms;
-    if (!host_mode) {
-        constexpr int R = ltlg_engine::RING;
-        DevCtl *rctl = (DevCtl *)e->h_ring.p;
-        DevLevel *rlev = (DevLevel *)((char *)e->h_ring.p + R * sizeof(DevCtl));
-        int enq = 0, done = 0;
-        // One graph for every level: planner and level kernel; the level kernel's last CTA
-        // writes the level's summary into ring slot (seq - 1) % R of the mapped host ring.
-        const long long key[8] = {tl, hk, pitch, block_threads, max_grid, 3, 0, 0};
-        if (memcmp(key, e->graph_key, sizeof(key)) != 0) {
-            memset(e->graph_key, 0, sizeof(e->graph_key));
-            if (e->level_graph[0]) cudaGraphExecDestroy(e->level_graph[0]);
-            e->level_graph[0] = nullptr;
-            cudaGraph_t g = nullptr;
-            err = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-            if (err == cudaSuccess) {
-                cudaError_t x = launch_plan(dA, st);
-                if (x == cudaSuccess) x = launch_level(A, dA, (int)max_grid, block_threads, st);
-                err = cudaStreamEndCapture(st, &g);
-                if (err == cudaSuccess) err = x;
-                if (err == cudaSuccess) err = cudaGraphInstantiate(&e->level_graph[0], g, 0);
-                if (g) cudaGraphDestroy(g);
-            }
-            if (err != cudaSuccess) return fail_cuda(e, err, res);
-            memcpy(e->graph_key, key, sizeof(key));
+    LoopOut o;
+    o.launches = 2;
+    o.last_cost = c1;
+    int shortage = -1;
+    bool last_round = false;
+    uint64_t all_before = all;
+    InstCtl *dctl = (InstCtl *)e->ctl.p;
+    const double tl = opt->time_limit_s;
+    if (persist) {
+        // ---- every level in one launch, planned on the device
+        if ((err = run_levels(e, true, e->grid, t0, tl, o)) != cudaSuccess) return fail_cuda(e, err, res);
+        if ((err = read_ctl(e, hc)) != cudaSuccess) return fail_cuda(e, err, res);
+        o.last_cost = std::max<int>(c1, (int)hc->last_cost);
+        if (hc->status & ST_FATAL) {
+            o.status = fatal_status(hc->status);
+        } else if (hc->found) {
+            o.found = true;
+        } else if (hc->flags & CTL_CANCELLED) {
+            o.status = LTLG_TIMEOUT;
+        } else if (hc->status & ST_OVERFLOW) {
+            // the level that overflowed ran to its end; continue after it on the host, check-only
+            o.on_the_fly = true;
+            shortage = (int)hc->overflow_cost;
         }
-        auto enqueue = [&]() -> cudaError_t {
-            const int k = enq % R;
-            cudaEventRecord(e->ev_start[k], st);
-            const cudaError_t x = cudaGraphLaunch(e->level_graph[0], st);
-            cudaEventRecord(e->ev_done[k], st);
-            launches += 2;
-            ++enq;
-            return x;
-        };
-        cudaEventRecord(e->ev_a, st);
-        while (enq < R - 1 && c1 + enq < max_cost)
-            if ((err = enqueue()) != cudaSuccess) return fail_cuda(e, err, res);
-        while (done < enq) {
-            const int k = done % R;
-            if ((err = cudaEventSynchronize(e->ev_done[k])) != cudaSuccess) return fail_cuda(e, err, res);
-            ++done;
-            const DevCtl &sc = rctl[k];
-            const DevLevel &sl = rlev[k];
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e->ev_start[k], e->ev_done[k]);
-            if (!sl.halt) level_ms.push_back(ms);
-            dflags |= sc.status;
-            bool stop = sl.halt != 0;
-            if (sc.status & fatal) {
-                status = fatal_status(sc.status);
-                stop = true;
-            } else if (sc.found && !found) {
-                found = true;
-                found_word = sc.found;
-                found_cost = (int)sc.found_cost;
-                if (opt->stop_at_found) {
-                    status = LTLG_FOUND;
-                    stop = true;
-                }
-            }
-            if (!stop && (sc.status & ST_OVERFLOW)) stop = true;
-            if (!sl.halt) last_cost = sl.cost;
-            if (sl.halt == 2) stop = true;
-            if (!stop && sl.cost >= max_cost) stop = true;
-            if (!stop && opt->time_limit_s > 0 && now_s() - t0 > opt->time_limit_s) {
-                status = LTLG_TIMEOUT;
-                stop = true;
-            }
-            if (stop) break;
-            if (c1 + enq < max_cost)
-                if ((err = enqueue()) != cudaSuccess) return fail_cuda(e, err, res);
-        }
-        cudaEventRecord(e->ev_b, st);
-        cudaMemcpyAsync(hc, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(hl, dlev, offsetof(DevLevel, blocks), cudaMemcpyDeviceToHost, st);
-        if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e->ev_a, e->ev_b);
-        device_ms += ms;
-        dflags |= hc->status;
-        if (status == LTLG_NOT_FOUND && !(hc->status & fatal) && ((hc->status & ST_OVERFLOW) || hl->halt == 2))
-            host_mode = true;
-        if (host_mode) {
-            if (hl->halt == 2) {
-                status = LTLG_BAD_ARGS;  // a level with more splits than a device plan holds
-                host_mode = false;
-            } else {
-                // the level that overflowed ran to its end; continue after it on the host
-                on_the_fly = true;
-                shortage = (int)hc->overflow_cost;
-                hl->cost = shortage;
-                hl->halt = 0;
-                hl->on_the_fly = 1;
-                cudaMemcpyAsync(dlev, hl, offsetof(DevLevel, blocks), cudaMemcpyHostToDevice, st);
-            }
-        }
+    } else {
+        if ((err = read_ctl(e, hc)) != cudaSuccess) return fail_cuda(e, err, res);
     }
 
     // ---- host-driven levels: the per-block schedule (per-block statistics, the reference's
     // progress lines) and the on-the-fly overflow regime (ltli6463.cu:1202-1206, 1442-1443).
-    if (host_mode && status == LTLG_NOT_FOUND && !(found && opt->stop_at_found)) {
-        uint64_t all_before = all;
+    // The plan of each level is made on the device (closed); the host opens it in windows.
+    const bool host_levels = (per_block || o.on_the_fly) && o.status == LTLG_NOT_FOUND && !o.found;
+    auto switch_on_the_fly = [&](int next_cost) -> cudaError_t {
+        A.on_the_fly = 1;
+        cudaError_t x = cudaMemcpyAsync(e->args.p, ha, sizeof(InstArgs), cudaMemcpyHostToDevice, st);
+        if (x != cudaSuccess) return x;
+        static const u32 zero = 0;
+        x = cudaMemcpyAsync(&dctl->flags, &zero, 4, cudaMemcpyHostToDevice, st);
+        if (x == cudaSuccess) x = launch_plan_level(dA, next_cost, st);
+        ++o.launches;
+        if (x == cudaSuccess) x = read_ctl(e, hc);
+        return x;
+    };
+    if (host_levels && o.on_the_fly)
+        if ((err = switch_on_the_fly((int)hc->last_cost + 1)) != cudaSuccess) return fail_cuda(e, err, res);
+    if (host_levels) {
+        const size_t W = sizeof(Entry);
         for (;;) {
-            const int cost = hl->cost + 1;
-            if (cost > max_cost) {
-                last_cost = max_cost;
-                break;
-            }
-            if (on_the_fly && shortage >= 0) {
+            if (hc->plan.halt || (hc->flags & CTL_DONE)) break;
+            const int cost = hc->plan.cost;
+            if (cost > max_cost) break;
+            if (o.on_the_fly && shortage >= 0) {
                 const int dif = cost - shortage;
                 if (dif == cf[1] || dif == c1 + cf[2] || dif == c1 + cf[3] || dif == cf[4] || dif == cf[5] ||
                     dif == cf[6] || dif == c1 + cf[7])
                     last_round = true;
             }
-            if ((err = launch_plan(dA, st)) != cudaSuccess) return fail_cuda(e, err, res);
-            ++launches;
-            cudaMemcpyAsync(hl, dlev, sizeof(DevLevel), cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(hc, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
-            if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
-            if (hl->halt) {
-                if (hl->halt == 2) status = LTLG_BAD_ARGS;  // more splits than a plan holds
-                last_cost = std::min(cost, max_cost);
-                break;
-            }
-            cudaEventRecord(e->ev_a, st);
-            DevCtl *dctl = (DevCtl *)e->ctl.p;
+            const u32 seq = hc->seq;
+            const int ne = hc->plan.nentries;
+            std::vector<int> order;
+            Entry *hent = (Entry *)e->h_entries.p;
             if (per_block) {
-                // one launch per block in the reference's order, each after a snapshot; the
-                // block's items are its window of the level's item table (unfused unary blocks)
-                size_t nb_level = 0;
-                for (int op = 0; op < 7; ++op) {
-                    for (int k = 0; k < hl->nblocks[op]; ++k) {
-                        cudaMemcpyAsync((DevCtl *)e->snaps.p + nb_level, e->ctl.p, sizeof(DevCtl),
-                                        cudaMemcpyDeviceToDevice, st);
-                        long long *win = (long long *)e->h_win.p + 8 * nb_level;
-                        long long lo = 0, hi = 0;
-                        block_window(hl, op, k, lo, hi);
-                        win[0] = lo;  // queue[0]
-                        win[1] = hi;  // items_end
-                        cudaMemcpyAsync(&dctl->queue[0], &win[0], sizeof(u64), cudaMemcpyHostToDevice, st);
-                        cudaMemcpyAsync(&dlev->items_end, &win[1], sizeof(long long), cudaMemcpyHostToDevice, st);
-                        const int grid = (int)std::max<long long>(1, std::min<long long>(hi - lo, max_grid));
-                        if ((err = launch_level(A, dA, grid, block_threads, st)) != cudaSuccess)
-                            return fail_cuda(e, err, res);
-                        ++launches;
-                        ++nb_level;
-                    }
-                }
-            } else {
-                if (hl->items_end > 0) {
-                    const int grid = (int)std::min<long long>(hl->items_end, max_grid);
-                    if ((err = launch_level(A, dA, grid, block_threads, st)) != cudaSuccess)
+                // one window per block, in the reference's order (unfused plans: an entry is a block)
+                cudaMemcpyAsync(hent, e->entries.p, (size_t)ne * W, cudaMemcpyDeviceToHost, st);
+                if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
+                for (int q = 0; q < ne; ++q) order.push_back(q);
+                std::sort(order.begin(), order.end(), [&](int a, int b) { return hent[a].pos < hent[b].pos; });
+                for (size_t q = 0; q < order.size(); ++q) {
+                    const Entry &E = hent[order[q]];
+                    cudaMemcpyAsync((u64 *)e->snaps.p + q, &dctl->row_count, 8, cudaMemcpyDeviceToDevice, st);
+                    if ((err = open_window(e, seq, E.item0, E.item0 + E.items, (int)q)) != cudaSuccess)
                         return fail_cuda(e, err, res);
-                    ++launches;
+                    const int grid = (int)std::max<long long>(1, std::min<long long>(E.items, e->grid));
+                    if ((err = run_levels(e, false, grid, t0, 0.0, o)) != cudaSuccess) return fail_cuda(e, err, res);
                 }
+                cudaMemcpyAsync(e->h_snaps.p, e->snaps.p, order.size() * 8, cudaMemcpyDeviceToHost, st);
+            } else {
+                if ((err = open_window(e, seq, 0, hc->plan.items, 0)) != cudaSuccess) return fail_cuda(e, err, res);
+                const int grid = (int)std::max<long long>(1, std::min<long long>(hc->plan.items, e->grid));
+                if ((err = run_levels(e, false, grid, t0, 0.0, o)) != cudaSuccess) return fail_cuda(e, err, res);
             }
-            cudaEventRecord(e->ev_b, st);
-            const u64 prev_rows = hc->row_count;
-            cudaMemcpyAsync(hc, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
-            size_t nsnap = 0;
-            for (int op = 0; op < 7; ++op) nsnap += (size_t)hl->nblocks[op];
-            if (per_block && nsnap)
-                cudaMemcpyAsync(e->h_snaps.p, e->snaps.p, nsnap * sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
-            if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
-            (void)prev_rows;
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e->ev_a, e->ev_b);
-            device_ms += ms;
-            dflags |= hc->status;
+            if ((err = read_ctl(e, hc)) != cudaSuccess) return fail_cuda(e, err, res);
             if (per_block) {
-                const DevCtl *sn = (const DevCtl *)e->h_snaps.p;
-                size_t q = 0;
+                const u64 *sn = (const u64 *)e->h_snaps.p;
                 uint64_t before = all_before;
-                for (int op = 0; op < 7; ++op)
-                    for (int k = 0; k < hl->nblocks[op]; ++k, ++q) {
-                        const BlockDesc &B = hl->blocks[op][k];
-                        ltlg_block_stat sb{};
-                        sb.cost = cost;
-                        sb.op = op;
-                        sb.left_cost = B.lcost;
-                        sb.right_cost = (op == OP_AND || op == OP_OR || op == OP_U) ? cost - B.lcost - cf[op + 1] : 0;
-                        sb.stored_before = std::min<long long>((long long)sn[q].row_count, cap_rows);
-                        sb.all_before = before;
-                        sb.to_check = B.candidates;
-                        before += (uint64_t)B.candidates;
-                        bstats.push_back(sb);
-                    }
+                for (size_t q = 0; q < order.size(); ++q) {
+                    const Entry &E = hent[order[q]];
+                    ltlg_block_stat sb{};
+                    sb.cost = cost;
+                    sb.op = E.kind == ENT_UNARY ? unary_slot_op(__builtin_ctz((unsigned)E.opmask)) : E.op;
+                    sb.left_cost = E.lcost;
+                    sb.right_cost = E.kind == ENT_UNARY ? 0 : E.rcost;
+                    sb.stored_before = std::min<long long>((long long)sn[q], cap_rows);
+                    sb.all_before = before;
+                    sb.to_check = (long long)E.cand;
+                    before += (uint64_t)E.cand;
+                    o.bstats.push_back(sb);
+                }
                 all_before = before;
             }
-            if (hc->status & fatal) {
-                status = fatal_status(hc->status);
-                last_cost = cost;
+            o.last_cost = cost;
+            if (hc->status & ST_FATAL) {
+                o.status = fatal_status(hc->status);
                 break;
             }
-            if (hc->found && !found) {
-                found = true;
-                found_word = hc->found;
-                found_cost = (int)hc->found_cost;
-                if (opt->stop_at_found) {
-                    status = LTLG_FOUND;
-                    break;
-                }
+            if (hc->found) {
+                o.found = true;
+                if (opt->stop_at_found) break;
             }
-            if (!on_the_fly && (hc->status & ST_OVERFLOW)) {
-                on_the_fly = true;
-                hl->on_the_fly = 1;
-                cudaMemcpyAsync(&dlev->on_the_fly, &hl->on_the_fly, sizeof(int), cudaMemcpyHostToDevice, st);
+            if (!o.on_the_fly && (hc->status & ST_OVERFLOW)) {
+                // switch to the on-the-fly regime: the next levels are check-only
+                o.on_the_fly = true;
+                if ((err = switch_on_the_fly(cost + 1)) != cudaSuccess) return fail_cuda(e, err, res);
             }
-            last_cost = cost;
             if (last_round) break;
-            if (on_the_fly && shortage == -1) shortage = cost;
-            if (opt->time_limit_s > 0 && now_s() - t0 > opt->time_limit_s) {
-                status = LTLG_TIMEOUT;
+            if (o.on_the_fly && shortage == -1) shortage = cost;
+            if (tl > 0 && now_s() - t0 > tl) {
+                o.status = LTLG_TIMEOUT;
                 break;
             }
         }
     }
 
-    // ---- level ranges, statistics, reference-style candidate count
-    cudaMemcpyAsync(e->h_ls.p, e->ls.p, (MAX_COSTS + 2) * sizeof(long long), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(e->h_lcands.p, e->lcands.p, (MAX_COSTS + 2) * sizeof(u64), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(hc, e->ctl.p, sizeof(DevCtl), cudaMemcpyDeviceToHost, st);
-    if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
+    // ---- level ranges, statistics, the reference's candidate count
+    cudaMemcpyAsync(e->h_ls.p, e->ls.p, (size_t)ncost * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(e->h_lcands.p, e->lcands.p, (size_t)ncost * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(e->h_lns.p, e->lns.p, (size_t)ncost * 8, cudaMemcpyDeviceToHost, st);
+    if ((err = read_ctl(e, hc)) != cudaSuccess) return fail_cuda(e, err, res);
     const long long rows_final = std::min<long long>((long long)hc->row_count, cap_rows);
     const long long *hls = (const long long *)e->h_ls.p;
     const u64 *hlc = (const u64 *)e->h_lcands.p;
-    const int top = found && opt->stop_at_found ? found_cost : std::max(last_cost, c1);
+    const u64 *hns = (const u64 *)e->h_lns.p;
+    const bool found = o.found || hc->found != 0;
+    const int found_cost = found ? (int)hc->found_cost : -1;
+    const u64 found_word = hc->found;
+    const bool stop_found = found && opt->stop_at_found;
+    const int top = stop_found ? found_cost : std::max(o.last_cost, c1);
     std::vector<long long> &ls = e->level_start;
     ls.assign((size_t)std::max(max_cost, c1) + 3, rows_final);
     for (int k = 0; k <= c1 && k < (int)ls.size(); ++k) ls[k] = 0;
     if (c1 + 1 < (int)ls.size()) ls[c1 + 1] = nalpha;
-    for (int k = c1 + 1; k <= std::min(top, MAX_COSTS) && k < (int)ls.size(); ++k) ls[k] = hls[k] > 0 ? hls[k] : ls[k];
-    for (int k = std::min(top, MAX_COSTS) + 1; k < (int)ls.size(); ++k) ls[k] = rows_final;
+    for (int k = c1 + 2; k <= top + 1 && k < (int)ls.size(); ++k) ls[k] = hls[k];
     std::vector<ltlg_level_stat> lstats;
+    u64 prev_ns = hc->t_start;
     for (int c = c1 + 1; c <= top && c + 1 < (int)ls.size(); ++c) {
         ltlg_level_stat L{};
         L.cost = c;
-        L.candidates = c <= MAX_COSTS ? hlc[c] : 0;
+        L.candidates = hlc[c];
         L.uniques = (uint64_t)(ls[c + 1] - ls[c]);
-        const size_t i = (size_t)(c - c1 - 1);
-        L.ms = i < level_ms.size() ? level_ms[i] : 0.0;
+        if (hns[c] && prev_ns) L.ms = (double)(hns[c] - prev_ns) * 1e-6;
+        if (hns[c]) prev_ns = hns[c];
         lstats.push_back(L);
     }
-    // all_ltls: whole levels before the found one, then the found level's blocks in the
-    // reference's order up to and including the block holding the find.
+    // all_ltls: whole levels before the level of the find, then that level's blocks in the
+    // reference's order up to and including the block the device recorded (the first block in
+    // that order that holds an accepting candidate, or with the learned order the one found).
     for (const auto &L : lstats)
-        if (!(found && opt->stop_at_found && L.cost == found_cost)) all += L.candidates;
-    if (found && opt->stop_at_found && found_word) {
-        const u64 p = found_word & ~(1ull << 63);
-        const int fop = parent_op(p);
-        int lc = cost_of_row(ls, (long long)parent_left(p));
-        if (fop == OP_U) lc = std::min(lc, cost_of_row(ls, (long long)parent_right(p)));
+        if (!(stop_found && L.cost == found_cost)) all += L.candidates;
+    if (stop_found && found_word) {
+        const u32 fpos = (u32)(hc->found_key & 0xFFFFFFFFull);
         std::vector<Block> blocks = level_blocks(found_cost, cf, opt->neg_type, ls);
-        for (const Block &B : blocks) {
-            all += (uint64_t)B.candidates;
-            if (B.op == fop && B.lcost == lc) break;
-        }
+        for (size_t q = 0; q < blocks.size() && q <= fpos; ++q) all += (uint64_t)blocks[q].candidates;
         if (per_block) {
             // drop the blocks after the one holding the find
             size_t keep = 0;
-            for (size_t i = 0; i < bstats.size(); ++i) {
+            int seen = 0;
+            for (size_t i = 0; i < o.bstats.size(); ++i) {
                 keep = i + 1;
-                if (bstats[i].cost == found_cost && bstats[i].op == fop && bstats[i].left_cost == lc) break;
+                if (o.bstats[i].cost == found_cost && seen++ == (int)fpos) break;
             }
-            bstats.resize(keep);
+            o.bstats.resize(keep);
         }
     }
+    int status = o.status;
     if (found && (status == LTLG_NOT_FOUND || status == LTLG_FOUND)) status = LTLG_FOUND;
+    if (status == LTLG_NOT_FOUND && (hc->flags & CTL_CANCELLED)) status = LTLG_TIMEOUT;
     res->status = status;
-    res->cost = found ? found_cost : last_cost;
+    res->cost = found ? found_cost : o.last_cost;
     res->all_ltls = all;
-    res->on_the_fly = on_the_fly ? 1 : 0;
-    res->device_flags = dflags;
-    res->device_ms = device_ms;
+    res->on_the_fly = o.on_the_fly ? 1 : 0;
+    res->device_flags = hc->status;
+    res->device_ms = o.device_ms;
     res->evaluated = (uint64_t)nalpha + hc->evaluated;
     res->rows = rows_final;
 
@@ -887,12 +831,14 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     if (letter_hit >= 0) {
         formula = std::string(1, alpha[letter_hit]);
         res->found_op = OP_ATOM;
+        res->cost = c1;
+        res->status = LTLG_FOUND;
     } else if (found && found_word) {
         const int wcap = 1024;
         if ((err = launch_walk((const u64 *)e->parents.p, nalpha, found_word, (u64 *)e->walk.p, wcap, st)) !=
             cudaSuccess)
             return fail_cuda(e, err, res);
-        ++launches;
+        ++o.launches;
         cudaMemcpyAsync(e->h_walk.p, e->walk.p, (2 + 2 * wcap) * 8, cudaMemcpyDeviceToHost, st);
         if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, res);
         const u64 *w = (const u64 *)e->h_walk.p;
@@ -914,14 +860,13 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         res->levels = (ltlg_level_stat *)malloc(sizeof(ltlg_level_stat) * lstats.size());
         memcpy(res->levels, lstats.data(), sizeof(ltlg_level_stat) * lstats.size());
     }
-    res->num_blocks = (int)bstats.size();
-    if (!bstats.empty()) {
-        res->blocks = (ltlg_block_stat *)malloc(sizeof(ltlg_block_stat) * bstats.size());
-        memcpy(res->blocks, bstats.data(), sizeof(ltlg_block_stat) * bstats.size());
+    res->num_blocks = (int)o.bstats.size();
+    if (!o.bstats.empty()) {
+        res->blocks = (ltlg_block_stat *)malloc(sizeof(ltlg_block_stat) * o.bstats.size());
+        memcpy(res->blocks, o.bstats.data(), sizeof(ltlg_block_stat) * o.bstats.size());
     }
-    res->launches = launches;
+    res->launches = o.launches;
     res->seconds = now_s() - t0;
-    (void)OPCH;
     return res->status;
 }
 
@@ -972,79 +917,90 @@ LTLG_API int ltlg_engine_label_blocks(ltlg_engine *e, const ltlg_traces *t, cons
     opt.stop_at_found = 1;
     opt.order = LTLG_ORDER_PLAIN;
     opt.schedule = LTLG_SCHEDULE_FUSED;
+    opt.record_levels = 2;  // row statistics for the features
     const int rc = ltlg_engine_learn(e, t, &opt, res);
     if (rc != LTLG_FOUND || res->found_op == OP_ATOM || res->on_the_fly) return rc;
     const int c = res->cost;
     const int *cf = opt.cost_fun;
     cudaStream_t st = e->stream;
-    const LevelArgs &A = *(const LevelArgs *)e->h_args.p;
-    const LevelArgs *dA = (const LevelArgs *)e->args.p;
+    InstArgs &A = *(InstArgs *)e->h_args.p;
+    const InstArgs *dA = (const InstArgs *)e->args.p;
     const std::vector<long long> &ls = e->level_start;
     if ((int)ls.size() < c + 2) return rc;
-    // Back to the start of level c: the rows of the lower levels (the level starts below c
-    // are still on the device), a clean control block, and a check-only plan of level c with
-    // one block per operator.
-    DevCtl *hc = (DevCtl *)e->h_ctl.p;
-    memset(hc, 0, sizeof(DevCtl));
-    hc->row_count = (u64)ls[c];
-    DevLevel *hl = (DevLevel *)e->h_lev.p;
-    memset(hl, 0, offsetof(DevLevel, blocks));
-    hl->cost = c - 1;
-    hl->on_the_fly = 1;
-    hl->plan_flags = PLAN_UNFUSED;
-    DevLevel *dlev = (DevLevel *)e->lev.p;
-    DevCtl *dctl = (DevCtl *)e->ctl.p;
-    cudaMemcpyAsync(dctl, hc, sizeof(DevCtl), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(dlev, hl, offsetof(DevLevel, blocks), cudaMemcpyHostToDevice, st);
-    cudaError_t err = launch_plan(dA, st);
-    if (err == cudaSuccess) err = cudaMemcpyAsync(hl, dlev, sizeof(DevLevel), cudaMemcpyDeviceToHost, st);
-    if (err == cudaSuccess)
-        err = cudaMemcpyAsync(e->h_lstats.p, e->lstats.p, (MAX_COSTS + 2) * LSTATS * sizeof(u64), cudaMemcpyDeviceToHost,
-                              st);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    // Back to the start of level c: the rows of the lower levels stay, the list of non-empty
+    // levels is cut at c, and level c is planned again with one entry per block, check-only
+    // (every candidate's acceptance is tested, nothing stored).
+    const long long ncost = (long long)e->max_cost + 3;
+    cudaError_t err = ensure_host(e->h_ne, (size_t)ncost * 4);
+    if (err == cudaSuccess) err = ensure_host(e->h_lstats, (size_t)ncost * LSTATS * 8);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(e->h_ne.p, e->ne.p, (size_t)ncost * 4, cudaMemcpyDeviceToHost, st);
+    InstCtl *hc = (InstCtl *)e->h_ctl.p;
+    if (err == cudaSuccess) err = read_ctl(e, hc);
     if (err != cudaSuccess) return fail_cuda(e, err, nullptr);
-    if (hl->halt) return rc;
-    const long long max_grid = (long long)e->num_sms *
-                               std::max(1, level_kernel_max_ctas_per_sm(A.left_tile, A.hash_kind, e->cfg.block_threads, A.pitch));
-    // One launch per block: clear the find, open the block's window, run, read the find.
-    long long *win = (long long *)e->h_win.p;
-    int nb = 0;
-    for (int op = 0; op < 7; ++op)
-        for (int k = 0; k < hl->nblocks[op]; ++k, ++nb) {
-            long long lo = 0, hi = 0;
-            block_window(hl, op, k, lo, hi);
-            long long *w = win + 8 * nb;
-            w[0] = lo;
-            w[1] = hi;
-            w[2] = 0;
-            cudaMemsetAsync(&dctl->found, 0, sizeof(u64), st);
-            cudaMemcpyAsync(&dctl->queue[0], &w[0], sizeof(u64), cudaMemcpyHostToDevice, st);
-            cudaMemcpyAsync(&dlev->items_end, &w[1], sizeof(long long), cudaMemcpyHostToDevice, st);
-            const int grid = (int)std::max<long long>(1, std::min<long long>(hi - lo, max_grid));
-            if ((err = launch_level(A, dA, grid, e->cfg.block_threads, st)) != cudaSuccess) return fail_cuda(e, err, nullptr);
-            cudaMemcpyAsync(&w[2], &dctl->found, sizeof(u64), cudaMemcpyDeviceToHost, st);
-        }
+    u32 nec = 0;
+    for (u32 q = 0; q < hc->ne_count; ++q)
+        if (((const int *)e->h_ne.p)[q] < c) nec = q + 1;
+    const u32 seq = hc->seq;
+    memset(hc, 0, sizeof(InstCtl));
+    hc->row_count = (u64)ls[c];
+    hc->found_key = NO_FIND;
+    hc->ne_count = nec;
+    hc->seq = seq;
+    hc->plan.cost = c - 1;
+    A.on_the_fly = 1;
+    A.plan_flags = PLAN_UNFUSED;
+    A.stop_at_found = 0;
+    A.find_first = 0;
+    cudaMemcpyAsync(e->ctl.p, hc, sizeof(InstCtl), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(e->args.p, &A, sizeof(InstArgs), cudaMemcpyHostToDevice, st);
+    err = launch_plan_level(dA, c, st);
+    if (err == cudaSuccess) err = read_ctl(e, hc);
+    if (err != cudaSuccess) return fail_cuda(e, err, nullptr);
+    if (hc->plan.halt || hc->plan.nentries <= 0) return rc;
+    const int ne = hc->plan.nentries, nbl = hc->plan.nblocks;
+    if ((err = ensure_host(e->h_fpar, (size_t)std::max(nbl, 1) * 8)) != cudaSuccess) return fail_cuda(e, err, nullptr);
+    Entry *hent = (Entry *)e->h_entries.p;
+    cudaMemcpyAsync(hent, e->entries.p, (size_t)ne * sizeof(Entry), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(e->h_lstats.p, e->lstats.p, (size_t)ncost * LSTATS * 8, cudaMemcpyDeviceToHost, st);
     if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, nullptr);
+    // One window per block: the block's accepting candidates record themselves at its position.
+    LoopOut o;
+    InstCtl *dctl = (InstCtl *)e->ctl.p;
+    static const u64 nofind = NO_FIND;
+    for (int q = 0; q < ne; ++q) {
+        const Entry &E = hent[q];
+        cudaMemcpyAsync(&dctl->found_key, &nofind, 8, cudaMemcpyHostToDevice, st);
+        if ((err = open_window(e, hc->seq, E.item0, E.item0 + E.items, q)) != cudaSuccess)
+            return fail_cuda(e, err, nullptr);
+        const int grid = (int)std::max<long long>(1, std::min<long long>(E.items, e->grid));
+        if ((err = run_levels(e, false, grid, now_s(), 0.0, o)) != cudaSuccess) return fail_cuda(e, err, nullptr);
+    }
+    cudaMemcpyAsync(e->h_fpar.p, e->fpar.p, (size_t)nbl * 8, cudaMemcpyDeviceToHost, st);
+    if ((err = cudaStreamSynchronize(st)) != cudaSuccess) return fail_cuda(e, err, nullptr);
+    const u64 *won = (const u64 *)e->h_fpar.p;
     const u64 *lst = (const u64 *)e->h_lstats.p;
-    int nbl = 0;
-    for (int q = 0; q < 7; ++q) nbl += hl->nblocks[q];
-    nb = 0;
+    std::vector<int> order(ne);
+    for (int q = 0; q < ne; ++q) order[q] = q;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return hent[a].pos < hent[b].pos; });
     int out = 0;
-    for (int op = 0; op < 7; ++op)
-        for (int k = 0; k < hl->nblocks[op]; ++k, ++nb) {
-            if (out >= cap) continue;
-            const BlockDesc &b = hl->blocks[op][k];
-            const BlockInfo bi = block_info(b, op, c, cf, nbl, (long long)hl->level_cands, lst, A.npos, A.n, A.nalpha);
-            ltlg_block_record &r = rec[out++];
-            r.cost = c;
-            r.op = op;
-            r.lcost = bi.lcost;
-            r.rcost = bi.rcost;
-            r.position = b.pad;
-            r.won = win[8 * nb + 2] != 0 ? 1 : 0;
-            r.candidates = b.candidates;
-            block_features(bi, r.features);
-        }
+    for (int q : order) {
+        if (out >= cap) break;
+        const Entry &E = hent[q];
+        const bool un = E.kind == ENT_UNARY;
+        const int op = un ? unary_slot_op(__builtin_ctz((unsigned)E.opmask)) : E.op;
+        const BlockInfo bi = block_info(op, c, E.lcost, un ? E.r1 - E.r0 : E.l1 - E.l0, un ? 1 : E.r1 - E.r0,
+                                        (long long)E.cand, E.pos, cf, nbl, (long long)hc->plan.cand, lst, e->max_cost,
+                                        A.npos, A.n, A.nalpha);
+        ltlg_block_record &r = rec[out++];
+        r.cost = c;
+        r.op = op;
+        r.lcost = bi.lcost;
+        r.rcost = bi.rcost;
+        r.position = E.pos;
+        r.won = (E.pos >= 0 && E.pos < nbl && won[E.pos] != 0) ? 1 : 0;
+        r.candidates = (long long)E.cand;
+        block_features(bi, r.features);
+    }
     *count = out;
     return rc;
 }
@@ -1057,9 +1013,7 @@ LTLG_API int ltlg_learn(const ltlg_traces *t, const ltlg_options *opt, ltlg_resu
     // them before its first device call (ltli6463.cu:1078-1083).
     if (t && opt && res && !traces_well_formed(t)) {
         memset(res, 0, sizeof(*res));
-        res->status = LTLG_BAD_ARGS;
-        res->formula = strdup(ltlg_status_string(LTLG_BAD_ARGS));
-        return res->status;
+        return fail_status(res, LTLG_BAD_ARGS);
     }
     if (t && opt && res && t->offsets && t->num_pos >= 0 && t->num_neg >= 0) {
         int max_len = 0;
@@ -1086,9 +1040,7 @@ LTLG_API int ltlg_learn(const ltlg_traces *t, const ltlg_options *opt, ltlg_resu
     int rc = ltlg_engine_create(&cfg, &e);
     if (rc != 0) {
         memset(res, 0, sizeof(*res));
-        res->status = rc;
-        res->formula = strdup(ltlg_status_string(rc));
-        return rc;
+        return fail_status(res, rc);
     }
     rc = ltlg_engine_learn(e, t, opt, res);
     ltlg_engine_destroy(e);
@@ -1197,7 +1149,8 @@ LTLG_API int ltlg_engine_hold_slot(ltlg_engine *e, const uint64_t *cs, int32_t n
         e->gen = 0;
     }
     // tag | the next learn's generation | "publication pending"
-    const u64 v = ((fp >> 40) << 40) | ((u64)(e->gen + 1) << 32) | 0xFFFFFFFFull;
+    static thread_local u64 v;
+    v = ((fp >> 40) << 40) | ((u64)(e->gen + 1) << 32) | 0xFFFFFFFFull;
     u64 *slot = (u64 *)e->slots.p + (fp & (e->nslots - 1));
     err = cudaMemcpyAsync(slot, &v, sizeof(v), cudaMemcpyHostToDevice, e->stream);
     if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);

@@ -1,4 +1,12 @@
 // Shared host/device definitions of the CS enumeration kernels.
+//
+// A learn is a sequence of cost levels.  Each level has a plan: its (operator, split) blocks,
+// cut into work items and listed in the order a device queue hands them out.  The level
+// kernel drains the queue; the warp that finishes the level's last item closes the level
+// (level starts, the find) and plans the next one on the device, so levels follow each other
+// inside one persistent launch.  One launch serves many independent instances the same way:
+// each instance has its own arguments, counters and plan, and the kernel's CTAs take items
+// from whichever instance has some.
 #pragma once
 
 #include <cstddef>
@@ -23,8 +31,10 @@ enum : u32 {
     ST_OVERFLOW = 1u,   // a new CS found no free cache row (the reference's onTheFly switch)
     ST_WAIT = 2u,       // a wait for a slot publication gave up
     ST_TABLE = 4u,      // hash set full
-    ST_TMA = 8u,        // a bulk copy did not complete in time
+    ST_TMA = 8u,        // a bulk copy or a pipeline wait did not complete in time
+    ST_STALL = 16u,     // no level progress for too long while waiting for the next plan
 };
+constexpr u32 ST_FATAL = ST_WAIT | ST_TABLE | ST_TMA | ST_STALL;
 
 // Parents of a row: op << 60 | left << 30 | right (rows < 2^30).
 __host__ __device__ inline u64 pack_parent(int op, u64 l, u64 r) { return ((u64)op << 60) | (l << 30) | r; }
@@ -32,148 +42,158 @@ __host__ __device__ inline int parent_op(u64 p) { return (int)((p >> 60) & 7); }
 __host__ __device__ inline u64 parent_left(u64 p) { return (p >> 30) & 0x3FFFFFFFull; }
 __host__ __device__ inline u64 parent_right(u64 p) { return p & 0x3FFFFFFFull; }
 
-struct DevCtl {
-    u64 row_count;   // rows handed out, letters included (may pass cap_rows on overflow)
-    u64 found;       // 0, or (1 << 63) | parents of an accepting candidate
-    u64 evaluated;   // candidates evaluated
-    u32 status;      // ST_* bits
-    u32 found_cost;  // level at which `found` was set
-    u32 overflow_cost;  // level at which the cache first overflowed
-    u32 ctas_done;   // CTAs of the running level-kernel launch that have finished (the last resets it)
-    u64 queue[8];    // next work item of each operator's kernel
-};
+// Operator of slot j of a fused unary entry: 0 ~, 1 X, 2 F, 3 G.
+__host__ __device__ inline int unary_slot_op(int j) { return j == 0 ? OP_NEG : j == 1 ? OP_X : j == 2 ? OP_F : OP_G; }
 
-// One (operator, split) block of a level.  Unary: source rows [r0, r1).
-// Binary: left rows [l0, l1) x right rows [r0, r1).
-struct BlockDesc {
-    int op;
-    int lcost;           // cost of the left operand (unary: of the operand)
-    int opmask;          // fused unary blocks: bit 0 ~, 1 X, 2 F, 3 G over the same source rows
-    int pad;             // position of the block in the reference's order within its level
-    long long l0, l1, r0, r1;
-    long long item0;     // first work item of this block within its operator
-    long long items;     // work items of this block
+constexpr int POS_NONE = 0x7FFFFFFF;
+constexpr int LSTATS = 2;              // row-statistics counters per cost (see count_row_stats)
+constexpr u64 NO_FIND = ~0ull;         // InstCtl::found_key before any find
+constexpr int SEQ_SHIFT = 40;          // InstCtl::claimed = plan sequence << 40 | next item
+constexpr u64 ITEM_MASK = (1ull << SEQ_SHIFT) - 1;
+
+enum : int { ENT_UNARY = 1, ENT_ANDOR = 2, ENT_U = 3 };
+
+// One entry of a level's plan, in queue order: one of the reference's (operator, split)
+// blocks, or (fused) every unary operator that reads the same source rows, so one load of a
+// source row serves all of them.
+struct Entry {
+    int kind;            // ENT_UNARY, ENT_ANDOR, ENT_U
+    int op;              // binary: OP_AND / OP_OR / OP_U; unary: 0
+    int opmask;          // unary: bit j = slot operator j (0 ~, 1 X, 2 F, 3 G)
+    int pos;             // position in the reference's block order (unary: the smallest of its operators)
+    int upos[4];         // unary: position of slot operator j's block, POS_NONE when absent
+    int lcost, rcost;    // operand costs (unary: lcost is the operand's, rcost 0)
+    long long l0, l1, r0, r1;  // binary: left rows [l0, l1) x right rows [r0, r1); unary: source rows [r0, r1)
+    long long item0;     // first queue item of the entry
+    long long items;     // queue items of the entry
     long long tiles_r;   // binary: right chunks per left tile
-    long long candidates;  // as the reference counts them (U: two per pair)
+    long long cand;      // candidates as the reference counts them (U: two per pair)
+    float score;         // learned order: the entry's sort key
+    int pad;
 };
 
-constexpr int MAX_SPLITS = 64;   // blocks per operator and level in a device-planned level
-constexpr int MAX_RANGES = 4 + 3 * MAX_SPLITS;  // entries of a level's item table
-constexpr int UNARY_ROWS = 1;    // source rows per warp in a unary item (each with every operator of its mask)
-constexpr int MAX_COSTS = 512;   // level starts kept on the device
-constexpr int LSTATS = 2;        // row-statistics counters per cost (see count_row_stats)
+// The header of a level's plan.
+struct Plan {
+    int cost;            // the level
+    int halt;            // 1: the search is over; nothing to run
+    int check_only;      // on-the-fly level: acceptance only, nothing stored
+    int nentries;        // entries, in queue order
+    int nblocks;         // blocks in the reference's order (positions 0 .. nblocks - 1)
+    int right_chunk;     // right rows per binary item
+    int unary_rows;      // source rows per unary item
+    int learned;         // 1: entries sorted by the scorer
+    long long items;     // queue items of the level
+    u64 cand;            // candidates of the level, counted as the reference counts them
+};
 
-// One entry of a level's item table: a block and where its items start.
-struct ItemRange {
-    long long item0;     // first item of the entry in the order the queue runs
-    long long plain0;    // the same item's number in the plain order
-    int cls;             // 1 unary (ublocks[idx]), 2 & or | (blocks[idx / MAX_SPLITS][idx % MAX_SPLITS]), 3 U
-    int idx;
+// The mutable state of one instance's learn (device memory).
+struct InstCtl {
+    u64 claimed;         // plan sequence << SEQ_SHIFT | next queue item
+    u64 limit;           // plan sequence << SEQ_SHIFT | end of the items handed out (the plan's items, or a window's end)
+    u64 done;            // items of the current plan (or window) finished; the level (window) ends at limit's item
+    u64 row_count;       // rows handed out, letters included (may pass cap_rows on overflow)
+    u64 found_key;       // smallest (cost << 32 | block position) of an accepting candidate; NO_FIND
+    u64 found;           // (1 << 63) | parents of the find, once the level of the find has ended
+    u64 evaluated;       // candidates evaluated
+    u32 status;          // ST_* bits
+    u32 found_cost;      // level of `found`
+    u32 overflow_cost;   // level at which the cache first overflowed (0: none)
+    u32 seq;             // plans published (the current plan is sequence seq)
+    u32 ne_count;        // non-empty levels so far (InstArgs::ne)
+    u32 last_cost;       // the last level that ran to its end
+    u32 flags;           // CTL_* bits
+    u32 pad;
+    u64 t_start;         // globaltimer when the first plan was published (ns)
+    Plan plan;           // the current level
+};
+enum : u32 {
+    CTL_DONE = 1u,       // the search ended (plan.halt): results are final
+    CTL_CANCELLED = 2u,  // it ended because the host's cancel flag was set (time limit)
 };
 
 enum : int {
-    PLAN_UNFUSED = 1,    // one unary block per operator (per-block runs, learned order, labels)
-    PLAN_LEARNED = 2,    // order the item table by the scorer (LevelArgs::model), highest first
+    PLAN_UNFUSED = 1,    // one unary entry per operator (per-block runs, labels)
+    PLAN_LEARNED = 2,    // the planner reorders each plan by the scorer (InstArgs::model)
 };
 
-// The plan of the level being enumerated, in device memory.  The planner kernel writes it
-// from the level starts; the host writes it directly in the per-block schedule.
-struct DevLevel {
-    int cost;            // the level being enumerated (the planner advances it)
-    int halt;            // 1: every operator kernel of this level exits at once
-    int check_only;      // on-the-fly: acceptance only, no dedupe, no storing
-    int on_the_fly;      // set by the host: plan check-only levels and ignore the overflow bit
-    int seq;             // planner runs since the learn started (the level's host ring slot is (seq - 1) % RING)
-    int pad0;
-    long long item_hi_all;  // all work items of the level
-    long long items_end;    // the level kernel takes items from ctl->queue[0] below it
-    int right_chunk;
-    int unary_rows;
-    int nblocks[8];
-    long long total_items[8];
-    long long item_hi[8];  // an operator kernel takes items from its queue until item_hi
-    u64 level_cands;     // candidates of the level, counted as the reference counts them
-    int plan_flags;      // set by the host: PLAN_* bits
-    int nublocks;        // unary blocks the level kernel works from (fused over operators
-                         // unless PLAN_UNFUSED)
-    BlockDesc ublocks[4];
-    BlockDesc blocks[7][MAX_SPLITS];
-    // The level's blocks in the order the queue runs: entry e covers queue items
-    // [ranges[e].item0, ranges[e + 1].item0) (the last one up to items_end).
-    int nranges;
-    int learned_order;   // 1: the table is sorted by score and the queue runs through it
-    ItemRange ranges[MAX_RANGES];
-    float scores[MAX_RANGES];  // learned order: each entry's sort key (chance of a find / sqrt(candidates))
-};
-
-static_assert(sizeof(DevCtl) % 8 == 0 && offsetof(DevLevel, blocks) % 8 == 0, "level summaries copy 8-byte words");
-
-struct LevelArgs {
-    // constant during a learn
+// The constant arguments of one instance's learn (device memory).
+struct InstArgs {
     int n;               // traces = words per CS
     int pitch;           // words per cache row (n rounded up to a multiple of 4)
     int npos;
     int nalpha;
     int key_mode;
     int rlx_type;        // KEY_REF: 0 exact pack, 1, 2, 3
-    u32 gen;             // hash-set generation (1..255)
     int stop_at_found;
-    int left_tile;
+    int find_first;      // 1: any find stops the level; 0: the first block of the reference's order that holds one
     int neg_type;
     int max_cost;
-    int nwarps;
+    int on_the_fly;      // plan check-only levels, ignore the overflow bit
+    int plan_flags;      // PLAN_* bits
     int cf[8];           // costs of p ~ & | X F G U
     int right_chunk_big, unary_rows_big;
-    int small_rows;      // small levels: right rows (unary: source-row pairs) per warp and item
-    int hash_kind;       // fingerprint kind of the operator kernels (0 multiply-add, 1 fmix64)
+    int small_rows;      // small levels: right rows (unary: source rows) per item
+    int tile;            // left rows staged per binary item (U: tile / 2 left rows)
+    u32 gen;             // hash-set generation (1..255)
+    int pad_;
+    long long small_level;  // levels with fewer candidates use small items
     long long wait_spins;   // polls (~128 ns apart) before a wait for a slot publication gives up
-    long long small_level;  // levels with fewer candidates use one row per warp per item
     long long cap_rows;
+    long long cap_entries;  // capacity of entries / found_par (entries holds twice that: the second half is scratch)
+    long long learn_min_items;  // PLAN_LEARNED: plans of at most this many items keep the plain order
+    u64 slot_mask;
     u64 *cache;
     u64 *parents;
     u64 *keys;           // 2 words per row for KEY_REF / KEY_HASH64, else null
     u64 *slots;
-    u64 slot_mask;
     const u64 *wmeta;    // per word: length mask | (positive << 63); 0 for padding
     const u32 *kmeta;    // KEY_REF: per word start | count << 16 | step << 24
-    DevCtl *ctl;
-    DevLevel *lev;
-    long long *ls;       // level starts: rows of cost c are [ls[c], ls[c + 1])
+    long long *ls;       // level starts, max_cost + 2 entries: rows of cost c are [ls[c], ls[c + 1])
+    int *ne;             // costs of the non-empty levels, increasing (InstCtl::ne_count of them)
     u64 *level_cands;    // per cost
-    const void *model;   // PLAN_LEARNED: the scorer (MlpDev)
+    u64 *level_ns;       // per cost: globaltimer when the level ended (or null)
     u64 *lstats;         // per cost, LSTATS counts of stored rows by their position-0 behaviour (or null)
-    void *ring;          // device view of the host's ring of level summaries (or null)
-    int ring_slots;
-    long long grid;      // CTAs of a level-kernel launch (a level of fewer items runs in one wave)
-    // per level (filled into the shared copy from the plan)
-    int cost;
-    int check_only;
-    int right_chunk;
-    int unary_rows;
+    Entry *entries;      // the current plan's entries
+    u64 *found_par;      // per block position of the current level: (1 << 63) | parents of an accepting candidate
+    InstCtl *ctl;
+    const void *model;   // PLAN_LEARNED: the scorer (MlpDev)
+    const volatile u32 *cancel;  // host-mapped flag (or null): when set, the next level boundary ends the search
 };
 
-// The feature inputs of block b (operator op) of level c: the same code on the device
-// (planner) and on the host (training records).  ls[k] is the first row of cost k; lstats
-// (or null) holds LSTATS row-statistics counters per cost.
-__host__ __device__ inline BlockInfo block_info(const BlockDesc &b, int op, int c, const int *cf, int nblocks,
-                                                long long level_cands, const u64 *lstats, int npos, int n,
-                                                int nalpha) {
+// A launch of the level kernel over one or more instances.
+struct Launch {
+    const InstArgs *args;    // per instance
+    int ninst;
+    int persist;             // 1: after a level, plan and run the next one in the same launch
+    int tile;                // left rows staged per binary item (U: tile / 2 left rows, two candidates each)
+    int stages;              // item slots in flight per CTA
+    long long tile_bytes;    // shared-memory bytes of one slot's tile
+};
+
+// The feature inputs of a block (operator op) of level c: the same code on the device
+// (scorer) and on the host (training records).  lstats (or null) holds LSTATS row-statistics
+// counters per cost, up to max_cost.
+__host__ __device__ inline BlockInfo block_info(int op, int c, int lcost, long long lrows, long long rrows,
+                                                long long cand, int position, const int *cf, int nblocks,
+                                                long long level_cands, const u64 *lstats, int max_cost, int npos,
+                                                int n, int nalpha) {
     const bool un = op == OP_NEG || op == OP_X || op == OP_F || op == OP_G;
     BlockInfo bi{};
     bi.op = op;
     bi.cost = c;
     bi.c1 = cf[0];
-    bi.lcost = b.lcost;
-    bi.rcost = un ? 0 : c - b.lcost - cf[op + 1];
-    bi.position = b.pad;
+    bi.lcost = lcost;
+    bi.rcost = un ? 0 : c - lcost - cf[op + 1];
+    bi.position = position;
     bi.nblocks = nblocks;
-    bi.lrows = un ? b.r1 - b.r0 : b.l1 - b.l0;
-    bi.rrows = un ? 1 : b.r1 - b.r0;
-    bi.candidates = b.candidates;
+    bi.lrows = lrows;
+    bi.rrows = un ? 1 : rrows;
+    bi.candidates = cand;
     bi.level_cands = level_cands;
     for (int k = 0; k < 2; ++k) {
-        bi.lstat[k] = (lstats && bi.lcost <= MAX_COSTS) ? (long long)lstats[(u64)bi.lcost * LSTATS + k] : 0ll;
-        bi.rstat[k] = (lstats && !un && bi.rcost <= MAX_COSTS) ? (long long)lstats[(u64)bi.rcost * LSTATS + k] : 0ll;
+        bi.lstat[k] = (lstats && bi.lcost >= 0 && bi.lcost <= max_cost) ? (long long)lstats[(u64)bi.lcost * LSTATS + k] : 0ll;
+        bi.rstat[k] =
+            (lstats && !un && bi.rcost >= 0 && bi.rcost <= max_cost) ? (long long)lstats[(u64)bi.rcost * LSTATS + k] : 0ll;
     }
     bi.npos = npos;
     bi.nneg = n - npos;
@@ -181,17 +201,22 @@ __host__ __device__ inline BlockInfo block_info(const BlockDesc &b, int op, int 
     return bi;
 }
 
-// Launch wrappers (ltl_kernels.cu).  A level is one kernel (launch_level) that drains
-// ctl->queue[0]; the planner (launch_plan) writes its plan first.  The kernels read their
-// arguments from `d`, a copy of `a` in device memory, so a captured graph stays valid while
-// `*d` changes; `a` (host) selects the template instance and the shared-memory size.
-int level_kernel_smem_bytes(int left_tile, int pitch);
-int level_kernel_max_ctas_per_sm(int left_tile, int hash_kind, int block, int pitch);
-cudaError_t launch_level(const LevelArgs &a, const LevelArgs *d, int grid, int block, cudaStream_t s);
-cudaError_t launch_plan(const LevelArgs *d, cudaStream_t s);
-cudaError_t launch_insert_letters(const LevelArgs &a, const LevelArgs *d, int nalpha, cudaStream_t s);
+// Shared memory of one CTA of the level kernel for `stages` slots of tile_bytes each.
+size_t level_kernel_smem(int stages, long long tile_bytes);
+// Threads per CTA of the level kernel (one producer warp and the consumer warps).
+constexpr int LEVEL_THREADS = 512;
+
+// Launch wrappers (learn.cu).  The kernels read their arguments from device memory, so a
+// launch (or a captured graph) stays valid while the arguments change between learns.
+cudaError_t launch_levels(const Launch &host_copy, const Launch *dev, int grid, int hash_kind, cudaStream_t s);
+cudaError_t launch_first_plan(const InstArgs *d, int ninst, int open, cudaStream_t s);
+cudaError_t launch_insert_letters(const InstArgs *d, int nalpha, int hash_kind, cudaStream_t s);
 cudaError_t launch_walk(const u64 *parents, int nalpha, u64 found, u64 *out, int cap, cudaStream_t s);
+// Plans level `cost` of the instance from its level starts (the levels below must be complete) and
+// publishes the plan closed: the host opens it (host-driven levels, block labels).
+cudaError_t launch_plan_level(const InstArgs *d, int cost, cudaStream_t s);
 cudaError_t launch_scorer_pack(const float *params, MlpDev *out, cudaStream_t s);
+int level_kernel_ctas_per_sm(int hash_kind, size_t smem);
 // prog: (op, arg) pairs in postfix, op OP_ATOM with arg = letter index; stack: depth x n words.
 cudaError_t launch_eval_formula(const int *prog, int len, const u64 *atoms, const u64 *lenmask, int n, u64 *stack,
                                 u64 *out, cudaStream_t s);

@@ -2,7 +2,7 @@
 // 32 -> 64 -> 64 -> 1 with ReLU, BF16 operands (inputs, weights, activations and the
 // backward products' gradient operands rounded to BF16) and FP32 products and sums.  The
 // gradient is that of the mean weighted binary cross-entropy with logits.  Every unit sums
-// its inputs in index order, as the planner's scorer does (mlp_score_warp in ltl_kernels.cu).
+// its inputs in index order, as the planner's scorer does (mlp_score_warp in score.cuh).
 //
 // The reference has no learned component; these kernels back the block ordering only.
 #include <cuda_bf16.h>
@@ -191,7 +191,26 @@ bool has_device() {
     return cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
 }
 
+// The scorer's device form from the packed FP32 parameters: weights rounded to BF16.
+__global__ void scorer_pack_kernel(const float *__restrict__ p, MlpDev *__restrict__ m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ORDER_H * ORDER_NF) m->w1[i] = __float2bfloat16(p[MLP_W1 + i]);
+    if (i < ORDER_H * ORDER_H) m->w2[i] = __float2bfloat16(p[MLP_W2 + i]);
+    if (i < ORDER_H) {
+        m->w3[i] = __float2bfloat16(p[MLP_W3 + i]);
+        m->b1[i] = p[MLP_B1 + i];
+        m->b2[i] = p[MLP_B2 + i];
+    }
+    if (i == 0) m->b3 = p[MLP_B3];
+}
+
 }  // namespace
+
+cudaError_t launch_scorer_pack(const float *params, MlpDev *out, cudaStream_t s) {
+    scorer_pack_kernel<<<(MLP_PARAMS + 255) / 256, 256, 0, s>>>(params, out);
+    return cudaGetLastError();
+}
+
 }  // namespace ltlg
 
 using namespace ltlg;

@@ -32,6 +32,7 @@ constexpr int NOALLOC_MAX_TRACES = 64;
 constexpr int NOALLOC_SLOTS_LOG2 = 18;                 // 2^18 eight-byte slots = 2 MiB
 constexpr int NOALLOC_MAX_DEVICES = 64;
 constexpr int WALK_CAP = 1024;
+constexpr int MAX_COSTS = 512;                         // max_cost stays below this (fixed level arrays)
 constexpr int NOALLOC_MIN_FORMULA = 16;                // holds "see_the_error", "not_found" and a letter
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
@@ -40,32 +41,31 @@ void *g_scratch_on[NOALLOC_MAX_DEVICES] = {};
 
 size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Rows of cost k are [ls[k], ls[k + 1]); the reference's block order (ltli6463.cu:1209-1440)
-// decides how many candidates the reference counts up to the block holding the find.
-unsigned long long count_to_found(int c, const int *cf, int neg_type, const long long *ls, int fop, int flc) {
+// Rows of cost k are [ls[k], ls[k + 1]); the candidates the reference counts in level c up to
+// and including the block at position fpos of its block order (ltli6463.cu:1209-1440), which
+// lists only blocks whose operand levels are non-empty.
+unsigned long long count_to_found(int c, const int *cf, int neg_type, const long long *ls, int fpos) {
     const int c1 = cf[0];
     unsigned long long all = 0;
-    bool hit = false;
-    auto size = [&](int k) { return (k >= 0 && k < c) ? ls[k + 1] - ls[k] : 0ll; };
-    auto take = [&](int op, int lc, long long n) {
-        if (hit || n <= 0) return;
+    int pos = 0;
+    auto size = [&](int k) { return (k >= c1 && k < c) ? ls[k + 1] - ls[k] : 0ll; };
+    auto take = [&](long long n) {
+        if (n <= 0 || pos > fpos) return;
         all += (unsigned long long)n;
-        if (op == fop && lc == flc) hit = true;
+        ++pos;
     };
-    if ((neg_type == 1 && c - cf[1] >= c1) || (neg_type == 2 && c - cf[1] == c1)) take(OP_NEG, c - cf[1], size(c - cf[1]));
-    for (int i = c1; 2 * i <= c - cf[2]; ++i) take(OP_AND, i, size(i) * size(c - i - cf[2]));
-    for (int i = c1; 2 * i <= c - cf[3]; ++i) take(OP_OR, i, size(i) * size(c - i - cf[3]));
-    if (c - cf[4] >= c1) take(OP_X, c - cf[4], size(c - cf[4]));
-    if (c - cf[5] >= c1) take(OP_F, c - cf[5], size(c - cf[5]));
-    if (c - cf[6] >= c1) take(OP_G, c - cf[6], size(c - cf[6]));
-    for (int i = c1; 2 * i <= c - cf[7]; ++i) take(OP_U, i, 2 * size(i) * size(c - i - cf[7]));
+    auto binary = [&](int cop, int mult) {
+        for (int i = c1; 2 * i <= c - cop; ++i)
+            if (size(i) > 0 && size(c - i - cop) > 0) take(mult * size(i) * size(c - i - cop));
+    };
+    if ((neg_type == 1 && c - cf[1] >= c1) || (neg_type == 2 && c - cf[1] == c1)) take(size(c - cf[1]));
+    binary(cf[2], 1);
+    binary(cf[3], 1);
+    if (c - cf[4] >= c1) take(size(c - cf[4]));
+    if (c - cf[5] >= c1) take(size(c - cf[5]));
+    if (c - cf[6] >= c1) take(size(c - cf[6]));
+    binary(cf[7], 2);
     return all;
-}
-
-int cost_of(const long long *ls, int top, long long row) {
-    for (int k = top; k >= 0; --k)
-        if (row >= ls[k] && row < ls[k + 1]) return k;
-    return -1;
 }
 
 struct Writer {
@@ -197,17 +197,22 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     unsigned char *base = (unsigned char *)g_scratch_on[dev];
 
     // Carve the scratch: fixed parts first, the language cache takes the rest.
+    const int max_cost = opt->max_cost;
+    const long long cap_entries = 4 + 3 * ((long long)max_cost / 2 + 2);
     size_t off = 0;
     auto carve = [&](size_t bytes) {
         unsigned char *p = base + off;
         off += up256(bytes);
         return p;
     };
-    DevCtl *ctl = (DevCtl *)carve(sizeof(DevCtl));
-    DevLevel *lev = (DevLevel *)carve(sizeof(DevLevel));
-    LevelArgs *dargs = (LevelArgs *)carve(sizeof(LevelArgs));
-    long long *ls = (long long *)carve((MAX_COSTS + 2) * sizeof(long long));
-    u64 *lcands = (u64 *)carve((MAX_COSTS + 2) * sizeof(u64));
+    InstCtl *ctl = (InstCtl *)carve(sizeof(InstCtl));
+    InstArgs *dargs = (InstArgs *)carve(sizeof(InstArgs));
+    Launch *dlaunch = (Launch *)carve(sizeof(Launch));
+    long long *ls = (long long *)carve((MAX_COSTS + 3) * sizeof(long long));
+    int *ne = (int *)carve((MAX_COSTS + 3) * sizeof(int));
+    u64 *lcands = (u64 *)carve((MAX_COSTS + 3) * sizeof(u64));
+    Entry *entries = (Entry *)carve((size_t)(2 * cap_entries) * sizeof(Entry));
+    u64 *fpar = (u64 *)carve((size_t)cap_entries * 8);
     u64 *wmeta = (u64 *)carve((size_t)pitch * 8);
     u32 *kmeta = (u32 *)carve((size_t)pitch * 4);
     u64 *walk = (u64 *)carve((2 + 2 * WALK_CAP) * 8);
@@ -224,6 +229,15 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     u64 *cache = (u64 *)carve((size_t)cap * pitch * 8);
     if (off > NOALLOC_SCRATCH_BYTES) return LTLG_NO_MEMORY;
 
+    // Level-kernel geometry: 8-row tiles of rows of at most 64 words, eight slots.
+    const int tile = 8, stages = 8;
+    const long long tile_bytes = (long long)tile * pitch * 8;
+    const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
+    int num_sms = 0;
+    cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+    const int per_sm = level_kernel_ctas_per_sm(hk, level_kernel_smem(stages, tile_bytes));
+    const int grid = (num_sms > 0 ? num_sms : 1) * (per_sm > 0 ? per_sm : 1);
+
     // Inputs and zeroed state (default stream, synchronous copies from stack arrays).
     u64 wm[NOALLOC_MAX_TRACES];
     memset(wm, 0, sizeof(wm));
@@ -231,83 +245,76 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
         const int ln = t->offsets[i + 1] - t->offsets[i];
         wm[i] = (ln >= 63 ? 0x7FFFFFFFFFFFFFFFull : ((1ull << ln) - 1)) | (i < npos ? (1ull << 63) : 0ull);
     }
-    DevCtl hc;
+    InstCtl hc;
     memset(&hc, 0, sizeof(hc));
     hc.row_count = (u64)nalpha;
-    int lev_head[4] = {c1, 0, 0, 0};  // cost, halt, check_only, on_the_fly
+    hc.found_key = NO_FIND;
+    hc.plan.cost = c1;
     if ((err = cudaMemcpy(cache, letters, (size_t)nalpha * pitch * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (err = cudaMemcpy(wmeta, wm, (size_t)pitch * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (err = cudaMemset(kmeta, 0, (size_t)pitch * 4)) != cudaSuccess ||
         (err = cudaMemset(slots, 0, nslots * 8)) != cudaSuccess ||
-        (err = cudaMemset(ls, 0, (MAX_COSTS + 2) * sizeof(long long))) != cudaSuccess ||
-        (err = cudaMemset(lcands, 0, (MAX_COSTS + 2) * sizeof(u64))) != cudaSuccess ||
-        (err = cudaMemset(lev, 0, offsetof(DevLevel, blocks))) != cudaSuccess ||
-        (err = cudaMemcpy(lev, lev_head, sizeof(lev_head), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (err = cudaMemset(ls, 0, (MAX_COSTS + 3) * sizeof(long long))) != cudaSuccess ||
+        (err = cudaMemset(lcands, 0, (MAX_COSTS + 3) * sizeof(u64))) != cudaSuccess ||
         (err = cudaMemcpy(ctl, &hc, sizeof(hc), cudaMemcpyHostToDevice)) != cudaSuccess)
         return LTLG_CUDA_ERROR;
 
-    int num_sms = 0;
-    cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
-    const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
-    const int block_threads = 256, tl = 8;
-    const int per_sm = level_kernel_max_ctas_per_sm(tl, hk, block_threads, pitch);
-    const long long max_grid = (long long)(num_sms > 0 ? num_sms : 1) * (per_sm > 0 ? per_sm : 1);
-
-    LevelArgs A;
+    InstArgs A;
     memset(&A, 0, sizeof(A));
     A.n = n;
     A.pitch = pitch;
     A.npos = npos;
     A.nalpha = nalpha;
     A.key_mode = opt->key_mode == LTLG_KEY_EXACT ? KEY_EXACT : KEY_HASH64;
-    A.gen = 1;  // the slots were just cleared
     A.stop_at_found = opt->stop_at_found ? 1 : 0;
-    A.left_tile = tl;
     A.neg_type = opt->neg_type;
-    A.max_cost = opt->max_cost;
-    A.nwarps = block_threads / 32;
+    A.max_cost = max_cost;
     for (int i = 0; i < 8; ++i) A.cf[i] = cf[i];
     A.right_chunk_big = 64;
     A.unary_rows_big = 64;
     A.small_rows = 1;
-    A.small_level = max_grid * 2048ll;
+    A.tile = tile;
+    A.gen = 1;  // the slots were just cleared
+    A.small_level = (long long)grid * 4 * tile * 64;
     A.wait_spins = 1ll << 22;
-    A.hash_kind = hk;
     A.cap_rows = cap;
+    A.cap_entries = cap_entries;
+    A.slot_mask = nslots - 1;
     A.cache = cache;
     A.parents = parents;
     A.keys = keys;
     A.slots = slots;
-    A.slot_mask = nslots - 1;
     A.wmeta = wmeta;
     A.kmeta = kmeta;
-    A.ctl = ctl;
-    A.lev = lev;
     A.ls = ls;
+    A.ne = ne;
     A.level_cands = lcands;
-    if ((err = cudaMemcpy(dargs, &A, sizeof(A), cudaMemcpyHostToDevice)) != cudaSuccess) return LTLG_CUDA_ERROR;
-    if ((err = launch_insert_letters(A, dargs, nalpha, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
+    A.entries = entries;
+    A.found_par = fpar;
+    A.ctl = ctl;
+    Launch L;
+    memset(&L, 0, sizeof(L));
+    L.args = dargs;
+    L.ninst = 1;
+    L.persist = 1;
+    L.tile = tile;
+    L.stages = stages;
+    L.tile_bytes = tile_bytes;
+    if ((err = cudaMemcpy(dargs, &A, sizeof(A), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (err = cudaMemcpy(dlaunch, &L, sizeof(L), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return LTLG_CUDA_ERROR;
+    if ((err = launch_insert_letters(dargs, nalpha, hk, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
+    // Every level in one launch: the level kernel plans each next level on the device.
+    if ((err = launch_first_plan(dargs, 1, 1, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
+    if ((err = launch_levels(L, dlaunch, grid, hk, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
+    if ((err = cudaMemcpy(&hc, ctl, sizeof(hc), cudaMemcpyDeviceToHost)) != cudaSuccess) return LTLG_CUDA_ERROR;
+    if (hc.status & (ST_WAIT | ST_TMA | ST_STALL)) return LTLG_DEVICE_WAIT;
+    if (hc.status & ST_TABLE) return LTLG_TABLE_FULL;
+    if ((hc.status & ST_OVERFLOW) && !(hc.found && opt->stop_at_found)) return LTLG_NO_MEMORY;
+    const int last_cost = (int)hc.last_cost > c1 ? (int)hc.last_cost : c1;
 
-    // Levels: planner, level kernel, then read the control record.
-    int last_cost = c1;
-    for (;;) {
-        if ((err = launch_plan(dargs, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
-        if ((err = launch_level(A, dargs, (int)max_grid, block_threads, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
-        int head[2];
-        if ((err = cudaMemcpy(&hc, ctl, sizeof(hc), cudaMemcpyDeviceToHost)) != cudaSuccess ||
-            (err = cudaMemcpy(head, lev, sizeof(head), cudaMemcpyDeviceToHost)) != cudaSuccess)
-            return LTLG_CUDA_ERROR;
-        if (hc.status & (ST_WAIT | ST_TMA)) return LTLG_DEVICE_WAIT;
-        if (hc.status & ST_TABLE) return LTLG_TABLE_FULL;
-        if (head[1] == 2) return LTLG_BAD_ARGS;  // more splits in a level than one plan holds
-        if (head[1] == 0) last_cost = head[0];
-        if (hc.found && opt->stop_at_found) break;
-        if (hc.status & ST_OVERFLOW) return LTLG_NO_MEMORY;
-        if (head[1] != 0 || head[0] >= opt->max_cost) break;
-    }
-
-    long long hls[MAX_COSTS + 2];
-    unsigned long long hlc[MAX_COSTS + 2];
+    long long hls[MAX_COSTS + 3];
+    unsigned long long hlc[MAX_COSTS + 3];
     if ((err = cudaMemcpy(hls, ls, sizeof(hls), cudaMemcpyDeviceToHost)) != cudaSuccess ||
         (err = cudaMemcpy(hlc, lcands, sizeof(hlc), cudaMemcpyDeviceToHost)) != cudaSuccess)
         return LTLG_CUDA_ERROR;
@@ -316,7 +323,7 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     const int top = stop_found ? (int)hc.found_cost : last_cost;
     for (int k = 0; k <= c1; ++k) hls[k] = 0;
     hls[c1 + 1] = nalpha;
-    for (int k = top + 1; k < MAX_COSTS + 2; ++k) hls[k] = rows;
+    for (int k = top + 2; k < MAX_COSTS + 3; ++k) hls[k] = rows;
     for (int c = c1 + 1; c < top; ++c) all += hlc[c];
     if (!stop_found) {
         // every level up to the last one ran to its end
@@ -329,14 +336,8 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
         }
         if (cost_out) *cost_out = (int)hc.found_cost;
     } else {
-        const u64 pf = hc.found & ~(1ull << 63);
-        const int fop = parent_op(pf);
-        int flc = cost_of(hls, top, (long long)parent_left(pf));
-        if (fop == OP_U) {
-            const int r = cost_of(hls, top, (long long)parent_right(pf));
-            flc = r < flc ? r : flc;
-        }
-        all += count_to_found(top, cf, opt->neg_type, hls, fop, flc);
+        // the reference's count: the level's blocks in order up to the one the device recorded
+        all += count_to_found(top, cf, opt->neg_type, hls, (int)(u32)(hc.found_key & 0xFFFFFFFFull));
         if (cost_out) *cost_out = top;
         if (all_ltls_out) *all_ltls_out = all;
     }

@@ -9,10 +9,14 @@ uniqueness in a 2^27-slot hash set — each solved to its minimal formula.
 Metric: unique CS per second (time-to-minimal-formula and candidate CS/s are
 reported beside it).  Each timed step runs the batch twice:
   - through the public batch call (ltlg_batch_learn: host traces in, formula strings
-    out, W engines on their own streams driven by native threads) — CUDA-event time
-    around the call gives ``e2e``;
-  - one instance at a time on one engine — the summed device time of the level
-    kernels (inputs already in HBM) gives ``value`` and the roofline.
+    out; one persistent launch whose instance slots take the instances from a device
+    queue) — CUDA-event time around the call gives ``e2e``;
+  - one instance at a time on one engine (one persistent launch per learn, inputs
+    already in HBM) — the summed device time of the launches gives ``value`` and the
+    roofline.
+After the timed steps the line also carries, each time-capped: the learned block order
+against the plain one (cfg5 shape), cfg1 against the reference's own binary, cfg3 exact
+against relaxed uniqueness, and cfg4's batched instances.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -50,8 +54,10 @@ def parse():
     ap.add_argument("--max-cost", type=int, default=500)
     ap.add_argument("--no-stop", action="store_true", help="enumerate every level up to --max-cost")
     ap.add_argument("--cache-gb", type=float, default=6.0, help="language cache per engine")
-    ap.add_argument("--workers", type=int, default=8,
-                    help="engines of the batch call; 0 times the single engine only (profiling runs)")
+    ap.add_argument("--slots", type=int, default=20,
+                    help="instance slots of the batch call; 0 times the single engine only (profiling runs)")
+    ap.add_argument("--slot-cache-gb", type=float, default=3.0, help="language cache per batch slot")
+    ap.add_argument("--slot-slots-log2", type=int, default=24, help="hash slots per batch slot")
     ap.add_argument("--slots-log2", type=int, default=27)
     ap.add_argument("--small-rows", type=int, default=1, help="small levels: right rows per warp and item")
     ap.add_argument("--right-chunk", type=int, default=16, help="large levels: right rows per binary item")
@@ -63,6 +69,7 @@ def parse():
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--quiet-extra", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-plain block order comparison")
+    ap.add_argument("--no-extras", action="store_true", help="skip the cfg1 / cfg3 / cfg4 objects of the line")
     ap.add_argument("--workload", choices=["cfg2", "cfg3", "cfg4"], default="cfg2",
                     help="cfg3: exact vs relaxed uniqueness on one large instance; cfg4: 4096 batched instances")
     ap.add_argument("--time-limit", type=float, default=120.0, help="cfg3: seconds per uniqueness mode")
@@ -231,7 +238,46 @@ def learned_order_report(ekw, repeats: int = 2):
                       if hard else None},
         "per_instance": [[r["cost_plain"], round(r["ms_plain"], 3), round(r["ms_learned"], 3)] for r in rows],
         "scorer": "scorer_hamming.npy: MLP 32-64-64-1, BF16/FP32, trained on the GPU on 198,070 block records",
+        "spec_shape": near_miss_report(ekw),
     }
+
+
+def near_miss_report(ekw, seeds=range(4), max_cost=8, time_limit_s=20.0):
+    """The cfg5 shape as specified: 4 props, 1000 random positives (len U[20,48], Bernoulli(0.5)),
+    1000 negatives = positives with 1-3 flipped bits (exact duplicates of positives rejected),
+    no planted formula.  Both orders enumerate every level up to max_cost (no separating formula
+    exists there), so the learned order has no level of a find to reorder."""
+    from ltlb200 import api, gen, learned
+    insts = [gen.generate_near_miss(s, 4, 1000, 1000, 20, 48, 0.5) for s in seeds]
+    kw = dict(ekw, slots_log2=max(ekw.get("slots_log2", 26), 26))
+    with api.Engine(**kw) as eng:
+        rows = learned.compare(eng, insts, learned.load_scorer(), repeats=1, max_cost=max_cost,
+                               time_limit_s=time_limit_s)
+    s = learned.summarize(rows)
+    return {"workload": f"4 props, 1000 random pos (len U[20,48], Bernoulli(0.5)) + 1000 negatives = positives "
+                        f"with 1-3 flipped bits, no planted formula; seeds {seeds[0]}-{seeds[-1]}; max_cost {max_cost}",
+            "found": sum(r["status_plain"] == api.FOUND for r in rows), "instances": s["instances"],
+            "same_cost": s["same_cost"], "time_ms": {"plain": s["ms_plain"], "learned": s["ms_learned"]},
+            "speedup": s["speedup"]}
+
+
+def extras(device: int, time_limit: float) -> dict:
+    """The cfg1 / cfg3 / cfg4 objects of the line (each skipped with its reason on failure)."""
+    from ltlb200 import workloads
+    out = {}
+    jobs = [("cfg1_vs_reference_binary",
+             lambda: workloads.run_cfg1(os.path.join(ROOT, "oracle", "_ref", "ltli6463_measure"),
+                                        os.path.join(ROOT, "tests", "golden", "inputs"))),
+            ("cfg3", lambda: workloads.run_cfg3(time_limit_s=time_limit, device=device)),
+            ("cfg4", lambda: workloads.run_cfg4(device=device))]
+    for key, job in jobs:
+        t0 = time.perf_counter()
+        try:
+            out[key] = job()
+        except Exception as exc:  # a failed extra must not lose the main line
+            out[key] = {"error": f"{type(exc).__name__}: {exc}"}
+        out[key]["wall_s"] = time.perf_counter() - t0
+    return out
 
 
 def run_reference(a):
@@ -300,7 +346,8 @@ def run_ours(a):
                right_chunk=a.right_chunk, unary_rows=a.unary_rows, left_tile=a.left_tile,
                block_threads=a.block_threads)
     eng = api.Engine(**ekw)
-    pool = api.Batch(workers=a.workers, **ekw) if a.workers > 0 else None
+    bkw = dict(ekw, cache_bytes=int(a.slot_cache_gb * (1 << 30)), slots_log2=a.slot_slots_log2)
+    pool = api.Batch(workers=a.slots, **bkw) if a.slots > 0 else None
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     opts = dict(neg_type=1, max_cost=a.max_cost, stop_at_found=not a.no_stop)
 
@@ -344,7 +391,7 @@ def run_ours(a):
                 uniq_e2e += r.rows - len(inst.alphabet)
                 cand_e2e += r.evaluated - len(inst.alphabet)
                 launches += r.launches
-                ttm.append(r.seconds * 1e3)
+                ttm.append(r.device_ms)
                 costs.append(r.cost)
                 h2d += len(inst.alphabet) * inst.n * 8 + inst.n * 12  # letter CSs + word metadata
                 d2h += len(r.formula) + 64
@@ -377,12 +424,15 @@ def run_ours(a):
             "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "seeds_per_rank": a.seeds, "instances_per_step": len(batch) * ws,
                        "l2": "flushed between timed steps (256 MiB write)",
-                       "parallelism": f"instances x{ws} ranks; {a.workers} engines per GPU in the batch call",
-                       "value": "unique CS / summed level-kernel device time, one instance at a time",
+                       "parallelism": f"instances x{ws} ranks; one persistent launch per GPU drains the batch "
+                                      f"through {a.slots} instance slots",
+                       "value": "unique CS / summed device time of the learns, one instance at a time "
+                                "(one persistent launch each)",
                        "e2e": "unique CS / CUDA-event time of ltlg_batch_learn on host traces"},
             "time_to_minimal_formula_ms": {"mean": statistics.mean(ttm), "median": statistics.median(ttm),
                                            "max": max(ttm), "min_cost": min(costs), "max_cost": max(costs),
-                                           "note": "host wall time of each learn inside the concurrent batch"},
+                                           "note": "device time of each instance inside the batch launch, "
+                                                   "from its slot's set-up to its result"},
             "candidate_cs_per_s": tot[3] / kern_t,
             "e2e": {"value": tot[0] / step_t, "unit": UNIT, "h2d_bytes_per_step": h2d // K,
                     "d2h_bytes_per_step": d2h // K, "candidate_cs_per_s": tot[1] / step_t},
@@ -392,9 +442,9 @@ def run_ours(a):
                          "alg_bytes_per_launch": alg_bytes / nl,
                          "kernel": "level_kernel", "bytes_per_unit": per_unit,
                          "units": "candidates evaluated + uniques stored",
-                         "timing": "level time from CUDA events on the engine stream around each level's graph "
-                                   "(planner + level kernel; the kernel writes the level summary into mapped "
-                                   "host memory), summed over the one-at-a-time pass",
+                         "timing": "CUDA events on the engine stream around each learn's persistent launch "
+                                   "(every level, the device planner included), summed over the "
+                                   "one-at-a-time pass",
                          "traffic_source": "ncu DRAM bytes per candidate of the cost-8 level_kernel launch "
                                            "(profiles/level_kernel_cfg2.txt) x mean candidates per launch"},
             "gpu_launches": launches,
@@ -404,6 +454,8 @@ def run_ours(a):
             line["learned_order"] = learned_order_report(ekw)
         if ws == 1 and not a.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(batch, a.cpu_sample_s)
+        if ws == 1 and not a.no_extras:
+            line.update(extras(local, a.time_limit))
         print(json.dumps(line), flush=True)
     if pool:
         pool.close()

@@ -89,26 +89,26 @@ typedef struct ltlg_engine_config {
     int64_t cache_bytes;       /* language-cache budget in bytes (rows = budget / (8 * pitch)) */
     int64_t max_rows;          /* upper bound on cache rows (<= 2^30); 0 = budget only */
     int32_t max_traces;        /* largest n the engine accepts */
-    int32_t block_threads;     /* threads per CTA of the level kernel (multiple of 32) */
+    int32_t block_threads;     /* kept for the layout; the level kernel runs one CTA of 512 threads
+                                  per SM (a producer warp and 15 consumer warps) */
     int32_t left_tile;         /* left rows staged in shared memory per binary work item: 2, 4 or 8 */
-    int32_t right_chunk;       /* right rows per binary work item */
-    int32_t unary_rows;        /* source rows per unary work item */
-    int32_t small_rows;        /* levels below the small-level size: right rows (unary: source-row
-                                  pairs) per warp and work item; 0 = 1 */
+    int32_t right_chunk;       /* right rows per binary work item of a large level */
+    int32_t unary_rows;        /* source rows per unary work item of a large level */
+    int32_t small_rows;        /* levels below the small-level size: right rows (unary: source rows)
+                                  per work item; 0 = 1 */
     int32_t wait_spins;        /* bound of a device wait for another warp's hash-slot publication, in
                                   polls about 128 ns apart; a wait that runs out ends the learn with
                                   LTLG_DEVICE_WAIT.  0 = 2^22 (about half a second) */
     int32_t pad_;
-    int64_t small_level;       /* levels with fewer candidates are cut into work items of one right row
-                                  (unary: one source row) per warp; larger levels use right_chunk /
-                                  unary_rows.  0 = 2048 x the level kernel's resident CTAs */
+    int64_t small_level;       /* levels with fewer candidates are cut into work items of small_rows
+                                  rows; larger levels use right_chunk / unary_rows.  0 = the size
+                                  below which large items would give fewer than four per CTA */
 } ltlg_engine_config;
 
 typedef struct ltlg_options {
     int32_t cost_fun[8];       /* p ~ & | X F G U, each in 1..SHRT_MAX */
-    int32_t max_cost;          /* levels up to min(max_cost, 511) are enumerated (the device keeps
-                                  511 level starts); a search that reaches 511 without a find
-                                  ends NOT_FOUND with cost 511 */
+    int32_t max_cost;          /* levels up to max_cost (1..SHRT_MAX, as the reference's maxCost) are
+                                  enumerated; level arrays and plans are sized for it per learn */
     int32_t rlx_unq_chk_type;  /* the reference's argument 11 (1, 2, 3), used with LTLG_KEY_REF */
     int32_t neg_type;          /* 1: negate every formula, 2: negate letters only (ltli6463.cu:1212) */
     int32_t key_mode;          /* ltlg_key_mode */
@@ -160,7 +160,7 @@ typedef struct ltlg_result {
 
 typedef struct ltlg_engine ltlg_engine;
 
-/* Defaults: device 0, 2^27 slots, 16 GiB cache, n <= 8192, 256 threads, left tile 4,
+/* Defaults: device 0, 2^27 slots, 16 GiB cache, n <= 8192, 512 threads, left tile 4,
    right chunk 16, unary rows 32, small rows 1, default wait bound and small-level size. */
 LTLG_API void ltlg_default_engine_config(ltlg_engine_config *cfg);
 /* The reference's defaults: unit costs, maxCost 500, type 3, NegType 2, exact keys, fused, plain. */
@@ -191,17 +191,24 @@ LTLG_API int ltlg_learn(const ltlg_traces *traces, const ltlg_options *opt, ltlg
  * formula text here, ltli6463.cu:1461, :1082, :984).  Accepts NULL. */
 LTLG_API void ltlg_result_free(ltlg_result *res);
 
-/* Batched learning: independent instances spread over `workers` engines (each with its own
- * stream and device buffers, driven by its own host thread), so the latency-bound small
- * levels of different instances overlap on the GPU.  results[i] belongs to traces[i];
- * free each with ltlg_result_free.  The reference has one instance per process
- * (code/dc.py:33-43 runs the binary once per sub-problem); this replaces that loop. */
+/* Batched learning: independent instances learned by one persistent launch of the level kernel.
+ * The batch holds `workers` instance slots, each with the buffers one engine of `cfg` would have
+ * (cache_bytes of language cache, 2^slots_log2 hash slots); the instances are uploaded at once and
+ * a device queue hands them to the slots: when an instance's search ends, the slot writes its
+ * result and takes the next pending instance, so the small levels of many instances run side by
+ * side and no host round trip happens between levels or instances.  results[i] belongs to
+ * traces[i]; free each with ltlg_result_free.  Instances with the reference's relaxed keys, the
+ * learned order, the per-block schedule or a time limit, and any instance whose slot's cache
+ * overflows, are learned one at a time on one engine of `cfg` instead.  The reference has one
+ * instance per process (code/dc.py:33-43 runs the binary once per sub-problem); this replaces
+ * that loop. */
 typedef struct ltlg_batch ltlg_batch;
 LTLG_API int ltlg_batch_create(const ltlg_engine_config *cfg, int32_t workers, ltlg_batch **out);
 LTLG_API void ltlg_batch_destroy(ltlg_batch *b);
 LTLG_API int ltlg_batch_learn(ltlg_batch *b, const ltlg_traces *traces, int32_t count, const ltlg_options *opt,
                               ltlg_result *results);
-/* Stream of worker w's engine (for event timing around batch calls). */
+/* The batch's stream (a cudaStream_t) for worker 0, NULL otherwise (for event timing around batch
+ * calls). */
 LTLG_API void *ltlg_batch_stream(ltlg_batch *b, int32_t worker);
 
 /* Learn without allocating: no counterpart in the reference.  For callers that cannot

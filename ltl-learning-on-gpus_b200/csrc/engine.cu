@@ -1047,22 +1047,70 @@ LTLG_API int ltlg_learn(const ltlg_traces *t, const ltlg_options *opt, ltlg_resu
     return rc;
 }
 
+// ---- Batches: the instance slots of one persistent launch (see BatchDev).  Instances that the
+// device batch does not take (the reference's relaxed keys, the learned order, the per-block
+// schedule, a time limit) and instances whose slot's cache overflowed are learned one by one on
+// a fallback engine with the same configuration.
 struct ltlg_batch {
-    std::vector<ltlg_engine *> engines;
+    ltlg_engine_config cfg{};
+    int slots = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    DevBuf cache, parents, keys, hslots, wmeta, kmeta, ls, ne, lcands, entries, fpar, ctl, args;
+    DevBuf bin, steps, offs, bout, cur, t0, bdev, launch;
+    DevBuf h_bin, h_steps, h_offs, h_bout, h_args, h_bdev, h_launch;
+    std::vector<u32> gen;          // each slot's hash-set generation after the last call
+    ltlg_engine *fallback = nullptr;
+    std::vector<float> scorer;     // set_scorer's parameters, for the fallback engine
 };
 
-LTLG_API int ltlg_batch_create(const ltlg_engine_config *cfg, int32_t workers, ltlg_batch **out) {
-    *out = nullptr;
-    if (workers < 1 || workers > 64) return LTLG_BAD_ARGS;
-    auto *b = new ltlg_batch();
-    for (int w = 0; w < workers; ++w) {
-        ltlg_engine *e = nullptr;
-        const int rc = ltlg_engine_create(cfg, &e);
+namespace {
+
+int batch_fallback(ltlg_batch *b, const ltlg_traces *t, const ltlg_options *opt, ltlg_result *res) {
+    if (!b->fallback) {
+        const int rc = ltlg_engine_create(&b->cfg, &b->fallback);
         if (rc != 0) {
-            ltlg_batch_destroy(b);
-            return rc;
+            memset(res, 0, sizeof(*res));
+            return fail_status(res, rc);
         }
-        b->engines.push_back(e);
+        if (!b->scorer.empty()) ltlg_engine_set_scorer(b->fallback, b->scorer.data(), (int32_t)b->scorer.size());
+    }
+    return ltlg_engine_learn(b->fallback, t, opt, res);
+}
+
+}  // namespace
+
+LTLG_API int ltlg_batch_create(const ltlg_engine_config *cfg_in, int32_t workers, ltlg_batch **out) {
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return LTLG_NO_DEVICE;
+    if (workers < 1 || workers > 4096) return LTLG_BAD_ARGS;
+    ltlg_engine_config cfg;
+    if (cfg_in)
+        cfg = *cfg_in;
+    else
+        ltlg_default_engine_config(&cfg);
+    if (cfg.device < 0 || cfg.device >= ndev || cfg.slots_log2 < 10 || cfg.slots_log2 > 34 ||
+        (cfg.left_tile != 2 && cfg.left_tile != 4 && cfg.left_tile != 8) || cfg.right_chunk < 1 ||
+        cfg.unary_rows < 1 || cfg.max_traces < 1 || cfg.wait_spins < 0 || cfg.small_level < 0 || cfg.cache_bytes < 64)
+        return LTLG_BAD_ARGS;
+    if (cfg.max_rows <= 0 || cfg.max_rows > (1ll << 30) - 1) cfg.max_rows = (1ll << 30) - 1;
+    auto *b = new ltlg_batch();
+    b->cfg = cfg;
+    b->slots = workers;
+    b->gen.assign(workers, 0u);
+    cudaError_t err = cudaSetDevice(cfg.device);
+    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, cfg.device);
+    if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    const size_t nslots = (size_t)1 << cfg.slots_log2;
+    const size_t cache_words = (size_t)cfg.cache_bytes / 8;
+    if (err == cudaSuccess) err = ensure(b->cache, (size_t)workers * cache_words * 8);
+    if (err == cudaSuccess) err = ensure(b->hslots, (size_t)workers * nslots * 8);
+    if (err == cudaSuccess) err = cudaMemsetAsync(b->hslots.p, 0, (size_t)workers * nslots * 8, b->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(b->stream);
+    if (err != cudaSuccess) {
+        ltlg_batch_destroy(b);
+        return err == cudaErrorMemoryAllocation ? LTLG_NO_MEMORY : LTLG_CUDA_ERROR;
     }
     *out = b;
     return 0;
@@ -1070,43 +1118,284 @@ LTLG_API int ltlg_batch_create(const ltlg_engine_config *cfg, int32_t workers, l
 
 LTLG_API void ltlg_batch_destroy(ltlg_batch *b) {
     if (!b) return;
-    for (ltlg_engine *e : b->engines) ltlg_engine_destroy(e);
+    cudaSetDevice(b->cfg.device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (DevBuf *x : {&b->cache, &b->parents, &b->keys, &b->hslots, &b->wmeta, &b->kmeta, &b->ls, &b->ne, &b->lcands,
+                      &b->entries, &b->fpar, &b->ctl, &b->args, &b->bin, &b->steps, &b->offs, &b->bout, &b->cur,
+                      &b->t0, &b->bdev, &b->launch})
+        if (x->p) cudaFree(x->p);
+    for (DevBuf *x : {&b->h_bin, &b->h_steps, &b->h_offs, &b->h_bout, &b->h_args, &b->h_bdev, &b->h_launch})
+        if (x->p) cudaFreeHost(x->p);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    ltlg_engine_destroy(b->fallback);
     delete b;
 }
 
 LTLG_API void *ltlg_batch_stream(ltlg_batch *b, int32_t worker) {
-    if (!b || worker < 0 || worker >= (int)b->engines.size()) return nullptr;
-    return (void *)b->engines[worker]->stream;
+    if (!b || worker != 0) return nullptr;
+    return (void *)b->stream;
 }
 
 LTLG_API int ltlg_batch_learn(ltlg_batch *b, const ltlg_traces *traces, int32_t count, const ltlg_options *opt,
                               ltlg_result *results) {
     if (!b || count < 0 || (count && (!traces || !results || !opt))) return LTLG_BAD_ARGS;
-    std::atomic<int> next{0};
-    auto work = [&](ltlg_engine *e) {
-        for (;;) {
-            const int i = next.fetch_add(1);
-            if (i >= count) return;
-            ltlg_engine_learn(e, &traces[i], opt, &results[i]);
+    const double t0 = now_s();
+    for (int i = 0; i < count; ++i) memset(&results[i], 0, sizeof(ltlg_result));
+    const int *cf = opt ? opt->cost_fun : nullptr;
+    bool opts_ok = opt != nullptr && opt->max_cost >= 1 && opt->max_cost <= SHRT_MAX && opt->key_mode >= 0 &&
+                   opt->key_mode <= 2 && (opt->order == LTLG_ORDER_PLAIN || opt->order == LTLG_ORDER_LEARNED);
+    for (int i = 0; opts_ok && i < 8; ++i)
+        if (cf[i] <= 0 || cf[i] > SHRT_MAX) opts_ok = false;
+    if (count && !opts_ok) {
+        for (int i = 0; i < count; ++i) fail_status(&results[i], LTLG_BAD_ARGS);
+        return LTLG_BAD_ARGS;
+    }
+    const bool device_batch = count > 0 && opt->key_mode != LTLG_KEY_REF && opt->order == LTLG_ORDER_PLAIN &&
+                              opt->schedule == LTLG_SCHEDULE_FUSED && opt->time_limit_s <= 0;
+    // which instances the device takes; the others are answered on the host or by the fallback
+    std::vector<int> dev_idx;
+    int min_pitch = INT_MAX, max_pitch = 4;
+    for (int i = 0; i < count; ++i) {
+        const ltlg_traces *t = &traces[i];
+        ltlg_result *r = &results[i];
+        const int n = t->num_pos + t->num_neg;
+        const int nalpha = t->alphabet ? (int)strlen(t->alphabet) : 0;
+        if (!traces_well_formed(t) || n > b->cfg.max_traces || nalpha > 26) {
+            fail_status(r, LTLG_BAD_ARGS);
+            continue;
         }
-    };
-    const int workers = std::min<int>((int)b->engines.size(), std::max(count, 1));
-    std::vector<std::thread> th;
-    for (int w = 1; w < workers; ++w) th.emplace_back(work, b->engines[w]);
-    work(b->engines[0]);
-    for (auto &t : th) t.join();
-    int rc = 0;
-    for (int i = 0; i < count; ++i)
-        if (results[i].status != LTLG_FOUND && results[i].status != LTLG_NOT_FOUND && !rc) rc = results[i].status;
+        int max_len = 0;
+        for (int q = 0; q < n; ++q) max_len = std::max(max_len, t->offsets[q + 1] - t->offsets[q]);
+        if ((opt->limit_traces && n > 64) || max_len > 63) {
+            r->status = LTLG_INPUT_LIMITS;
+            r->cost = cf[0];
+            r->formula = strdup("see_the_error");
+            continue;
+        }
+        if (!device_batch) {
+            batch_fallback(b, t, opt, r);
+            continue;
+        }
+        const int pitch = std::max(4, (n + 3) & ~3);
+        min_pitch = std::min(min_pitch, pitch);
+        max_pitch = std::max(max_pitch, pitch);
+        dev_idx.push_back(i);
+    }
+    const int nd = (int)dev_idx.size();
+    cudaError_t err = cudaSuccess;
+    if (nd > 0) {
+        err = cudaSetDevice(b->cfg.device);
+        const int K = std::min(b->slots, nd);
+        const int max_cost = opt->max_cost;
+        const long long ncost = (long long)max_cost + 3;
+        const long long cap_entries = entries_for(max_cost);
+        const long long cache_words = b->cfg.cache_bytes / 8;
+        const long long max_rows = std::min<long long>(b->cfg.max_rows, cache_words / min_pitch);
+        const bool keyed = opt->key_mode != LTLG_KEY_EXACT;
+        const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
+        int tile = 0, stages = 0;
+        long long tile_bytes = 0;
+        if (!geometry(b->cfg.left_tile, max_pitch, tile, stages, tile_bytes)) err = cudaErrorInvalidValue;
+        const int per_sm = err == cudaSuccess ? level_kernel_ctas_per_sm(hk, level_kernel_smem(stages, tile_bytes)) : 0;
+        if (per_sm < 1 && err == cudaSuccess) err = cudaErrorInvalidConfiguration;
+        const int grid = b->num_sms * std::max(per_sm, 1);
+        // inputs: instance records, steps and offsets of every instance in one array each
+        long long total_steps = 0, total_offs = 0;
+        for (int i : dev_idx) {
+            const ltlg_traces *t = &traces[i];
+            const int n = t->num_pos + t->num_neg;
+            total_steps += n ? t->offsets[n] - t->offsets[0] : 0;
+            total_offs += n + 1;
+        }
+        const size_t bout_bytes = (size_t)nd * sizeof(BatchOut);
+        auto dev = [&](DevBuf &x, size_t bytes) {
+            if (err == cudaSuccess) err = ensure(x, std::max<size_t>(bytes, 16));
+        };
+        auto host = [&](DevBuf &x, size_t bytes) {
+            if (err == cudaSuccess) err = ensure_host(x, std::max<size_t>(bytes, 16));
+        };
+        dev(b->parents, (size_t)K * max_rows * 8);
+        if (keyed) dev(b->keys, (size_t)K * max_rows * 16);
+        dev(b->wmeta, (size_t)K * max_pitch * 8);
+        dev(b->kmeta, (size_t)K * max_pitch * 4);
+        dev(b->ls, (size_t)K * ncost * 8);
+        dev(b->lcands, (size_t)K * ncost * 8);
+        dev(b->ne, (size_t)K * ncost * 4);
+        dev(b->entries, (size_t)K * 2 * cap_entries * sizeof(Entry));
+        dev(b->fpar, (size_t)K * cap_entries * 8);
+        dev(b->ctl, (size_t)K * sizeof(InstCtl));
+        dev(b->args, (size_t)K * sizeof(InstArgs));
+        dev(b->cur, (size_t)K * 4);
+        dev(b->t0, (size_t)K * 8);
+        dev(b->bin, (size_t)nd * sizeof(BatchIn));
+        dev(b->steps, (size_t)total_steps * 4);
+        dev(b->offs, (size_t)total_offs * 4);
+        dev(b->bout, bout_bytes);
+        dev(b->bdev, sizeof(BatchDev));
+        dev(b->launch, sizeof(Launch));
+        host(b->h_bin, (size_t)nd * sizeof(BatchIn));
+        host(b->h_steps, (size_t)total_steps * 4);
+        host(b->h_offs, (size_t)total_offs * 4);
+        host(b->h_bout, bout_bytes);
+        host(b->h_args, (size_t)K * sizeof(InstArgs));
+        host(b->h_bdev, sizeof(BatchDev));
+        host(b->h_launch, sizeof(Launch));
+        if (err == cudaSuccess) {
+            BatchIn *bi = (BatchIn *)b->h_bin.p;
+            u32 *hs = (u32 *)b->h_steps.p;
+            int *ho = (int *)b->h_offs.p;
+            long long sp = 0, op = 0;
+            for (int q = 0; q < nd; ++q) {
+                const ltlg_traces *t = &traces[dev_idx[q]];
+                const int n = t->num_pos + t->num_neg;
+                BatchIn &x = bi[q];
+                memset(&x, 0, sizeof(x));
+                x.npos = t->num_pos;
+                x.nneg = t->num_neg;
+                x.nalpha = t->alphabet ? (int)strlen(t->alphabet) : 0;
+                if (x.nalpha) memcpy(x.alpha, t->alphabet, (size_t)x.nalpha);
+                x.steps0 = sp;
+                x.offs0 = op;
+                const int base = n ? t->offsets[0] : 0;
+                for (int k = 0; k <= n; ++k) ho[op + k] = n ? t->offsets[k] - base : 0;
+                const long long ns = n ? t->offsets[n] - base : 0;
+                if (ns) memcpy(hs + sp, t->steps + base, (size_t)ns * 4);
+                sp += ns;
+                op += n + 1;
+            }
+            // slot arguments: the slot's buffers and the learn's options (set-up fills the rest)
+            InstArgs *ha = (InstArgs *)b->h_args.p;
+            const u64 nslots = 1ull << b->cfg.slots_log2;
+            for (int s2 = 0; s2 < K; ++s2) {
+                InstArgs &A = ha[s2];
+                memset(&A, 0, sizeof(A));
+                A.key_mode = keyed ? KEY_HASH64 : KEY_EXACT;
+                A.stop_at_found = opt->stop_at_found ? 1 : 0;
+                A.neg_type = opt->neg_type;
+                A.max_cost = max_cost;
+                for (int q = 0; q < 8; ++q) A.cf[q] = cf[q];
+                A.right_chunk_big = b->cfg.right_chunk;
+                A.unary_rows_big = b->cfg.unary_rows;
+                A.small_rows = std::max(1, b->cfg.small_rows);
+                A.tile = tile;
+                A.gen = b->gen[s2];
+                A.small_level = b->cfg.small_level > 0 ? b->cfg.small_level
+                                                       : (long long)grid * 4 * tile * std::max(1, b->cfg.right_chunk);
+                A.wait_spins = b->cfg.wait_spins > 0 ? b->cfg.wait_spins : (1ll << 22);
+                A.cap_entries = cap_entries;
+                A.learn_min_items = (long long)grid * stages;
+                A.slot_mask = nslots - 1;
+                A.cache = (u64 *)b->cache.p + (size_t)s2 * cache_words;
+                A.parents = (u64 *)b->parents.p + (size_t)s2 * max_rows;
+                A.keys = keyed ? (u64 *)b->keys.p + (size_t)s2 * max_rows * 2 : nullptr;
+                A.slots = (u64 *)b->hslots.p + (size_t)s2 * nslots;
+                A.wmeta = (const u64 *)b->wmeta.p + (size_t)s2 * max_pitch;
+                A.kmeta = (const u32 *)b->kmeta.p + (size_t)s2 * max_pitch;
+                A.ls = (long long *)b->ls.p + (size_t)s2 * ncost;
+                A.ne = (int *)b->ne.p + (size_t)s2 * ncost;
+                A.level_cands = (u64 *)b->lcands.p + (size_t)s2 * ncost;
+                A.entries = (Entry *)b->entries.p + (size_t)s2 * 2 * cap_entries;
+                A.found_par = (u64 *)b->fpar.p + (size_t)s2 * cap_entries;
+                A.ctl = (InstCtl *)b->ctl.p + s2;
+            }
+            BatchDev &D = *(BatchDev *)b->h_bdev.p;
+            memset(&D, 0, sizeof(D));
+            D.in = (const BatchIn *)b->bin.p;
+            D.steps = (const u32 *)b->steps.p;
+            D.offs = (const int *)b->offs.p;
+            D.out = (BatchOut *)b->bout.p;
+            D.args = (InstArgs *)b->args.p;
+            D.cur = (int *)b->cur.p;
+            D.t0 = (u64 *)b->t0.p;
+            D.cache_words = cache_words;
+            D.max_rows = max_rows;
+            D.count = nd;
+            D.nslots = K;
+            D.max_pitch = max_pitch;
+            Launch &L = *(Launch *)b->h_launch.p;
+            memset(&L, 0, sizeof(L));
+            L.args = (const InstArgs *)b->args.p;
+            L.batch = (BatchDev *)b->bdev.p;
+            L.ninst = K;
+            L.persist = 1;
+            L.tile = tile;
+            L.stages = stages;
+            L.tile_bytes = tile_bytes;
+            cudaStream_t st = b->stream;
+            err = cudaMemcpyAsync(b->bin.p, b->h_bin.p, (size_t)nd * sizeof(BatchIn), cudaMemcpyHostToDevice, st);
+            if (err == cudaSuccess && total_steps)
+                err = cudaMemcpyAsync(b->steps.p, b->h_steps.p, (size_t)total_steps * 4, cudaMemcpyHostToDevice, st);
+            if (err == cudaSuccess)
+                err = cudaMemcpyAsync(b->offs.p, b->h_offs.p, (size_t)total_offs * 4, cudaMemcpyHostToDevice, st);
+            if (err == cudaSuccess)
+                err = cudaMemcpyAsync(b->args.p, ha, (size_t)K * sizeof(InstArgs), cudaMemcpyHostToDevice, st);
+            if (err == cudaSuccess) err = cudaMemsetAsync(b->ctl.p, 0, (size_t)K * sizeof(InstCtl), st);
+            if (err == cudaSuccess) err = cudaMemcpyAsync(b->bdev.p, &D, sizeof(BatchDev), cudaMemcpyHostToDevice, st);
+            if (err == cudaSuccess) err = cudaMemcpyAsync(b->launch.p, &L, sizeof(Launch), cudaMemcpyHostToDevice, st);
+            if (err == cudaSuccess) err = launch_batch_start((BatchDev *)b->bdev.p, K, hk, st);
+            if (err == cudaSuccess) err = launch_levels(L, (const Launch *)b->launch.p, grid, hk, st);
+            if (err == cudaSuccess) err = cudaMemcpyAsync(b->h_bout.p, b->bout.p, bout_bytes, cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess)
+                err = cudaMemcpyAsync(ha, b->args.p, (size_t)K * sizeof(InstArgs), cudaMemcpyDeviceToHost, st);
+            if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+            if (err == cudaSuccess)
+                for (int s2 = 0; s2 < K; ++s2) b->gen[s2] = ha[s2].gen;
+        }
+        // results
+        const BatchOut *bo = (const BatchOut *)b->h_bout.p;
+        const double wall = now_s() - t0;
+        for (int q = 0; q < nd; ++q) {
+            const int i = dev_idx[q];
+            ltlg_result *r = &results[i];
+            if (err != cudaSuccess) {
+                r->status = LTLG_CUDA_ERROR;
+                r->formula = strdup(cudaGetErrorString(err));
+                continue;
+            }
+            const BatchOut &o = bo[q];
+            if (o.status == LTLG_NO_MEMORY) {  // its slot's cache overflowed: learn it alone
+                batch_fallback(b, &traces[i], opt, r);
+                continue;
+            }
+            const std::string alpha = traces[i].alphabet ? traces[i].alphabet : "";
+            r->status = o.status;
+            r->cost = o.cost;
+            r->all_ltls = o.all_ltls;
+            r->evaluated = o.evaluated;
+            r->rows = o.rows;
+            r->device_flags = o.device_flags;
+            r->device_ms = (double)o.ns * 1e-6;
+            r->seconds = wall;
+            r->launches = 2;
+            std::string formula;
+            if (o.letter >= 0 && o.letter < (int)alpha.size()) {
+                formula = std::string(1, alpha[o.letter]);
+                r->found_op = OP_ATOM;
+            } else if (o.status == LTLG_FOUND && o.found) {
+                r->found_op = parent_op(o.found & ~(1ull << 63));
+                if (o.walk_overflow || o.walk_count - 1 >= 200) {
+                    formula = "Size of the output is too big";
+                } else {
+                    std::map<u64, u64> par;
+                    for (int k = 1; k < o.walk_count; ++k) par[o.walk[2 * k]] = o.walk[2 * k + 1];
+                    build_string(par, ~0ull, o.found & ~(1ull << 63), true, alpha, (int)alpha.size(), formula, 0);
+                }
+            } else {
+                formula = ltlg_status_string(o.status);
+            }
+            r->formula = strdup(formula.c_str());
+        }
+    }
+    int rc = err != cudaSuccess ? LTLG_CUDA_ERROR : 0;
+    for (int i = 0; i < count && !rc; ++i)
+        if (results[i].status != LTLG_FOUND && results[i].status != LTLG_NOT_FOUND) rc = results[i].status;
     return rc;
 }
 
 LTLG_API int ltlg_batch_set_scorer(ltlg_batch *b, const float *params, int32_t count) {
-    if (!b) return LTLG_BAD_ARGS;
-    for (ltlg_engine *e : b->engines) {
-        const int rc = ltlg_engine_set_scorer(e, params, count);
-        if (rc != 0) return rc;
-    }
+    if (!b || !params || count != MLP_PARAMS) return LTLG_BAD_ARGS;
+    b->scorer.assign(params, params + count);
+    if (b->fallback) return ltlg_engine_set_scorer(b->fallback, params, count);
     return 0;
 }
 

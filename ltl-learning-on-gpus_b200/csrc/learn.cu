@@ -34,6 +34,7 @@
 // Every device wait is bounded; giving up sets a status bit the host reads.
 #include <atomic>
 
+#include "ltlgpu.h"
 #include "ops.cuh"
 #include "score.cuh"
 
@@ -53,7 +54,6 @@ constexpr u64 STALL_NS = 4000000000ull;        // no level progress while waitin
 struct Slot {
     u64 full;                 // mbarrier: the producer filled the slot (and its tile landed)
     u64 empty;                // mbarrier: every consumer left the slot
-    const InstArgs *A;        // the item's instance
     long long row0;           // binary: first right row; unary: first source row
     long long l_first;        // binary: first left row of the tile
     long long plan_items;     // items of the plan: the item done that brings `done` to it ends the level
@@ -69,6 +69,10 @@ struct Slot {
     int cost;
     int check_only;
     int stop;                 // remaining rows are skipped (a find at or before this entry)
+    int inst;                 // the item's instance (index into Launch::args)
+    int pad;
+    InstArgs args;            // its arguments as they were when the item was claimed (a batch slot's
+                              // arguments change when it takes the next instance)
 };
 
 // ---------------------------------------------------------------- candidate generators
@@ -800,7 +804,7 @@ __device__ __forceinline__ void publish(InstCtl *C, long long items, bool open) 
 // stopping when the search is over.  Levels without any block are closed on the spot.  One
 // warp (all lanes).  With open false (host-driven levels) the next plan is made but hands out
 // nothing until the host opens it.
-__device__ void close_level(const InstArgs &A, InstCtl *C, bool open, int lane) {
+__device__ bool close_level(const InstArgs &A, InstCtl *C, bool open, int lane) {
     __threadfence();
     int c = (int)__ldcg(&C->plan.cost);
     bool halt = false;
@@ -835,7 +839,7 @@ __device__ void close_level(const InstArgs &A, InstCtl *C, bool open, int lane) 
                 publish(C, 0, false);
             }
             __syncwarp();
-            return;
+            return true;
         }
         ++c;
         plan_level(A, C, c, lane);
@@ -844,9 +848,323 @@ __device__ void close_level(const InstArgs &A, InstCtl *C, bool open, int lane) 
         if (items > 0) {
             if (lane == 0) publish(C, items, open);
             __syncwarp();
-            return;
+            return false;
         }
         // a level without blocks: it ends where it starts
+    }
+}
+
+// ---------------------------------------------------------------- batches
+// Candidates the reference counts in level c up to and including the block at position fpos of
+// its block order (ltli6463.cu:1209-1440; only blocks whose operand levels are non-empty have
+// positions).  Lane 0.
+__device__ u64 count_blocks_through(const InstArgs &A, int c, int fpos) {
+    const int c1 = A.cf[0];
+    u64 all = 0;
+    int pos = 0;
+    auto size = [&](int k) -> long long { return (k >= c1 && k < c) ? ls_at(A, k + 1) - ls_at(A, k) : 0ll; };
+    auto take = [&](long long n) {
+        if (n <= 0 || pos > fpos) return;
+        all += (u64)n;
+        ++pos;
+    };
+    auto binary = [&](int cop, long long mult) {
+        for (int i = c1; 2 * i <= c - cop; ++i) {
+            const long long a = size(i), b = size(c - i - cop);
+            if (a > 0 && b > 0) take(mult * a * b);
+        }
+    };
+    const int *cf = A.cf;
+    if ((A.neg_type == 1 && c - cf[1] >= c1) || (A.neg_type == 2 && c - cf[1] == c1)) take(size(c - cf[1]));
+    binary(cf[2], 1);
+    binary(cf[3], 1);
+    if (c - cf[4] >= c1) take(size(c - cf[4]));
+    if (c - cf[5] >= c1) take(size(c - cf[5]));
+    if (c - cf[6] >= c1) take(size(c - cf[6]));
+    binary(cf[7], 2);
+    return all;
+}
+
+__device__ __forceinline__ void load_args(InstArgs &A, const InstArgs *src) {
+    constexpr int AW = sizeof(InstArgs) / 8;
+    for (int w = 0; w < AW; ++w) reinterpret_cast<u64 *>(&A)[w] = __ldcg(reinterpret_cast<const u64 *>(src) + w);
+}
+
+// The result of slot s's instance, as ltlg_engine_learn reports it: status, cost, the
+// reference's candidate count, and the found candidate's tree (row, parents) breadth first.
+// One warp; lane 0 writes.
+__device__ void finish_instance(BatchDev &B, int s, int lane) {
+    if (lane == 0) {
+        InstArgs A;
+        load_args(A, B.args + s);
+        InstCtl *C = A.ctl;
+        const int idx = B.cur[s];
+        BatchOut &o = B.out[idx];
+        const int c1 = A.cf[0];
+        const u32 st = __ldcg(&C->status), flags = __ldcg(&C->flags);
+        const u64 found = __ldcg(&C->found);
+        const int found_cost = (int)__ldcg(&C->found_cost);
+        const int last_cost = max(c1, (int)__ldcg(&C->last_cost));
+        const int letter = __ldcg(&o.letter);
+        int status = LTLG_NOT_FOUND;
+        if (st & ST_FATAL)
+            status = (st & ST_TABLE) ? LTLG_TABLE_FULL : LTLG_DEVICE_WAIT;
+        else if (found || letter >= 0)
+            status = LTLG_FOUND;
+        else if (flags & CTL_CANCELLED)
+            status = LTLG_TIMEOUT;
+        else if (st & ST_OVERFLOW)
+            status = LTLG_NO_MEMORY;  // the slot's cache overflowed: the host learns it alone
+        const bool stop_found = found && A.stop_at_found;
+        const int top = stop_found ? found_cost : last_cost;
+        u64 all = (u64)A.nalpha;
+        for (int c = c1 + 1; c <= top; ++c)
+            if (!(stop_found && c == found_cost)) all += __ldcg(A.level_cands + c);
+        if (stop_found) all += count_blocks_through(A, found_cost, (int)(u32)__ldcg(&C->found_key));
+        o.status = status;
+        o.cost = letter >= 0 ? c1 : found ? found_cost : last_cost;
+        o.all_ltls = all;
+        o.evaluated = (u64)A.nalpha + __ldcg(&C->evaluated);
+        o.rows = min((long long)__ldcg(&C->row_count), A.cap_rows);
+        o.found = letter >= 0 ? 0ull : found;
+        o.device_flags = st;
+        o.ns = globaltimer() - B.t0[s];
+        // the tree of the find, breadth first (entry 0 is the root)
+        int count = 0, overflow = 0;
+        if (found && letter < 0) {
+            u64 *e = o.walk;
+            e[0] = ~0ull;
+            e[1] = found & ~(1ull << 63);
+            count = 1;
+            for (int head = 0; head < count && !overflow; ++head) {
+                const u64 p = e[2 * head + 1];
+                const int op = parent_op(p);
+                const u64 kids[2] = {parent_left(p), parent_right(p)};
+                const int nk = (op == OP_AND || op == OP_OR || op == OP_U) ? 2 : (op == OP_ATOM ? 0 : 1);
+                for (int q = 0; q < nk; ++q) {
+                    if (kids[q] < (u64)A.nalpha) continue;
+                    if (count >= WALK_MAX) {
+                        overflow = 1;
+                        break;
+                    }
+                    e[2 * count] = kids[q];
+                    e[2 * count + 1] = __ldcg(A.parents + kids[q]);
+                    ++count;
+                }
+            }
+        }
+        o.walk_count = count;
+        o.walk_overflow = overflow;
+        __threadfence();
+    }
+    __syncwarp();
+}
+
+// Sets slot s up with instance idx: letters (the first separating one may end the search here,
+// ltli6463.cu:1100-1136), word metadata, the slot's next hash-set generation, a clean control
+// block and level arrays, the letters in the hash set, then the first plan.  One warp.  Returns
+// true when the instance's levels run; false when its search ended at set-up (result written).
+template <int HK>
+__device__ bool setup_instance(BatchDev &B, int s, int idx, int lane) {
+    BatchIn in;
+    {
+        const u64 *src = reinterpret_cast<const u64 *>(B.in + idx);
+        for (int w = 0; w < (int)(sizeof(BatchIn) / 8); ++w) reinterpret_cast<u64 *>(&in)[w] = __ldcg(src + w);
+    }
+    InstArgs A;
+    load_args(A, B.args + s);
+    InstCtl *C = A.ctl;
+    BatchOut &o = B.out[idx];
+    const int npos = in.npos, n = in.npos + in.nneg, nalpha = in.nalpha;
+    const int pitch = n <= 4 ? 4 : ((n + 3) & ~3);
+    const int c1 = A.cf[0];
+    if (lane == 0) {
+        B.cur[s] = idx;
+        B.t0[s] = globaltimer();
+        o.letter = -1;
+        o.walk_count = 0;
+        o.walk_overflow = 0;
+        o.found = 0;
+    }
+    const u32 *steps = B.steps + in.steps0;
+    const int *offs = B.offs + in.offs0;
+    // letters: rows 0 .. nalpha - 1, positives need position 0, negatives must not hold there
+    int hit = -1;
+    u64 all = 0;
+    for (int j = 0; j < nalpha; ++j) {
+        const u32 bit = 1u << (in.alpha[j] - 'a');
+        bool acc = true;
+        for (int i = lane; i < pitch; i += 32) {
+            u64 w = 0;
+            if (i < n) {
+                const int a = offs[i], b = offs[i + 1];
+                for (int k = a; k < b; ++k)
+                    if (steps[k] & bit) w |= 1ull << (k - a);
+                if (i < npos ? !(w & 1ull) : (w & 1ull)) acc = false;
+            }
+            __stcg(A.cache + (u64)j * pitch + i, w);
+        }
+        acc = __all_sync(FULL, acc);
+        ++all;
+        if (acc && hit < 0) {
+            hit = j;
+            if (A.stop_at_found) break;
+        }
+    }
+    if (hit >= 0 && lane == 0) o.letter = hit;
+    if ((hit >= 0 && A.stop_at_found) || n == 0 || nalpha == 0) {
+        if (lane == 0) {
+            o.status = hit >= 0 ? LTLG_FOUND : LTLG_NOT_FOUND;
+            o.cost = hit >= 0 ? c1 : max(c1, A.max_cost);
+            o.all_ltls = all;
+            o.evaluated = all;
+            o.rows = hit >= 0 ? hit + 1 : 0;
+            o.device_flags = 0;
+            o.ns = globaltimer() - B.t0[s];
+            __threadfence();
+        }
+        __syncwarp();
+        return false;
+    }
+    // word metadata: length mask | positive flag
+    for (int i = lane; i < pitch; i += 32) {
+        u64 m = 0;
+        if (i < n) {
+            const int ln = offs[i + 1] - offs[i];
+            m = (ln >= 63 ? 0x7FFFFFFFFFFFFFFFull : ((1ull << ln) - 1)) | (i < npos ? (1ull << 63) : 0ull);
+        }
+        __stcg(const_cast<u64 *>(A.wmeta) + i, m);
+    }
+    // the slot's arguments for this instance; a generation that wraps clears the set
+    A.n = n;
+    A.pitch = pitch;
+    A.npos = npos;
+    A.nalpha = nalpha;
+    A.rlx_type = 0;
+    A.on_the_fly = 0;
+    A.cap_rows = min(B.max_rows, B.cache_words / pitch);
+    if (A.gen >= 255) {
+        for (u64 q = lane; q <= A.slot_mask; q += 32) __stcg(A.slots + q, 0ull);
+        A.gen = 1;
+    } else {
+        A.gen += 1;
+    }
+    {
+        constexpr int AW = sizeof(InstArgs) / 8;
+        for (int w = lane; w < AW; w += 32)
+            __stcg(reinterpret_cast<u64 *>(B.args + s) + w, reinterpret_cast<const u64 *>(&A)[w]);
+    }
+    // level arrays and the control block (the plan sequence goes on: claim tags stay unique)
+    for (int k = lane; k <= A.max_cost + 2; k += 32) {
+        __stcg(A.ls + k, 0ll);
+        __stcg(A.level_cands + k, 0ull);
+    }
+    if (lane == 0) {
+        const u32 seq = __ldcg(&C->seq);
+        C->claimed = (u64)seq << SEQ_SHIFT;
+        C->limit = (u64)seq << SEQ_SHIFT;
+        C->done = 0;
+        C->row_count = (u64)nalpha;
+        C->found_key = NO_FIND;
+        C->found = 0;
+        C->evaluated = 0;
+        C->status = 0;
+        C->found_cost = 0;
+        C->overflow_cost = 0;
+        C->ne_count = 0;
+        C->last_cost = 0;
+        C->flags = 0;
+        C->t_start = globaltimer();
+        C->plan.cost = c1;
+        C->plan.halt = 0;
+    }
+    __threadfence();
+    __syncwarp();
+    // the letters into the hash set, in letter order (a duplicate letter stays a row, the set
+    // keeps the first, as the reference's sequential inserts do: ltli6463.cu:1134, :1189-1190)
+    const int nch = pitch >> 1;
+    const u64 tagmask = ~((1ull << 40) - 1);
+    for (int j = 0; j < nalpha; ++j) {
+        const ulonglong2 *row = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)j * pitch);
+        u64 h[1] = {0};
+        for (int c = lane; c < nch; c += 32) {
+            const u64 k = (2ull * (u64)c + 1ull) * WEYL;
+            const ulonglong2 w = __ldcg(row + c);
+            h[0] += hw<HK>(w.x, k, 2 * c < n) + hw<HK>(w.y, k + WEYL, 2 * c + 1 < n);
+        }
+        const u64 fp = fmix64(reduce_to_lane<1>(h, lane));
+        const u64 tagbits = fp & tagmask, genbits = (u64)A.gen << 32;
+        u64 idx2 = fp & A.slot_mask;
+        for (u64 probe = 0; probe <= A.slot_mask; ++probe, idx2 = (idx2 + 1) & A.slot_mask) {
+            u64 v = 0;
+            int action = 0;  // 0 next, 1 claimed, 2 compare
+            if (lane == 0) {
+                v = ld_acquire(A.slots + idx2);
+                if (slot_free(v, A.gen)) {
+                    const u64 old = atomicCAS(A.slots + idx2, v, tagbits | genbits | (u64)(j + 1));
+                    if (old == v)
+                        action = 1;
+                    else
+                        v = old;
+                }
+                if (action == 0 && (v & tagmask) == tagbits && (u32)v < FIELD_OVERFLOW) action = 2;
+            }
+            action = __shfl_sync(FULL, action, 0);
+            v = __shfl_sync(FULL, v, 0);
+            if (action == 1) break;
+            if (action == 2) {
+                const u64 other = (u64)(u32)v - 1;
+                bool same;
+                if (A.key_mode == KEY_EXACT) {
+                    bool diff = false;
+                    const ulonglong2 *ex = reinterpret_cast<const ulonglong2 *>(A.cache + other * pitch);
+                    for (int c = lane; c < nch; c += 32) {
+                        const ulonglong2 a = __ldcg(row + c), b = __ldcg(ex + c);
+                        diff |= (a.x != b.x) | (a.y != b.y);
+                    }
+                    same = !__any_sync(FULL, diff);
+                } else {
+                    same = __ldcg(A.keys + 2 * other) == fp;
+                }
+                if (same) break;
+            }
+        }
+        if (lane == 0) {
+            A.parents[j] = pack_parent(OP_ATOM, 0, 0);
+            if (A.keys) {
+                A.keys[2 * j] = fp;
+                A.keys[2 * j + 1] = 0;
+            }
+        }
+        __threadfence();
+        __syncwarp();
+    }
+    // the first plan: the letters' level has just ended
+    const bool ended = close_level(A, C, true, lane);
+    if (ended) finish_instance(B, s, lane);
+    return !ended;
+}
+
+// Slot s takes pending instances until one has levels to run or none is left.  `live` counts the
+// slots whose instance is searching: a slot that was searching (finishing) keeps its count when it
+// takes another instance and drops it when none is left; a slot starting out adds it.  One warp.
+template <int HK>
+__device__ __noinline__ void next_instance(BatchDev &B, int s, bool finishing, int lane) {
+    if (finishing) finish_instance(B, s, lane);
+    for (;;) {
+        u64 j = 0;
+        if (lane == 0) j = atomicAdd(&B.next, 1ull);
+        j = __shfl_sync(FULL, j, 0);
+        if (j >= (u64)B.count) {
+            if (finishing && lane == 0) atomicSub(&B.live, 1);
+            __syncwarp();
+            return;
+        }
+        if (setup_instance<HK>(B, s, (int)j, lane)) {
+            if (!finishing && lane == 0) atomicAdd(&B.live, 1);
+            __syncwarp();
+            return;
+        }
     }
 }
 
@@ -855,11 +1173,11 @@ __device__ __forceinline__ Slot *slot_at(unsigned char *smem, int s) { return re
 
 // Item `item` of entry e (cached in shared memory) into slot sl.  Returns the tile bytes to copy
 // (0 for a unary item or a skipped one).
-__device__ __forceinline__ u32 fill_slot(Slot &sl, const InstArgs *A, const Entry &e, long long item, int tile,
-                                         int rc, int ur, int cost, int check_only, long long plan_items, bool skip,
+__device__ __forceinline__ u32 fill_slot(Slot &sl, int inst, const Entry &e, long long item, int tile, int rc,
+                                         int ur, int cost, int check_only, long long plan_items, bool skip,
                                          int pitch) {
     const long long local = item - e.item0;
-    sl.A = A;
+    sl.inst = inst;
     sl.kind = e.kind;
     sl.pos = e.pos;
     for (int j = 0; j < 4; ++j) sl.upos[j] = e.upos[j];
@@ -898,7 +1216,24 @@ struct ProdCache {
     long long plan_items;
     long long item0[ENTRY_CACHE];
     Entry e;
+    InstArgs a;           // the instance's arguments (read once per plan)
 };
+
+__device__ __forceinline__ InstCtl *ctl_of(const Launch &L, int inst) { return (InstCtl *)__ldcg((const u64 *)&L.args[inst].ctl); }
+
+// Every instance of the launch is finished (a batch: no instance pending and no slot searching).
+__device__ __forceinline__ bool launch_done(const Launch &L, int lane) {
+    if (L.batch) {
+        bool d = true;
+        if (lane == 0)
+            d = ld_volatile(&L.batch->next) >= (u64)L.batch->count && *(volatile int *)&L.batch->live == 0;
+        return __shfl_sync(FULL, d, 0);
+    }
+    bool all_done = true;
+    for (int q = lane; q < L.ninst; q += 32)
+        if (!(*(volatile u32 *)&ctl_of(L, q)->flags & CTL_DONE)) all_done = false;
+    return __all_sync(FULL, all_done);
+}
 
 // The producer warp: claims items, fills slots, issues the tile copies and the L2 prefetches.
 template <int TL>
@@ -923,7 +1258,7 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
             if (lane == 0) ok = mbar_wait_for(&sl.empty, (u32)(((k / S) - 1) & 1), EMPTY_WAIT_NS);
             ok = __shfl_sync(FULL, ok, 0);
             if (!ok) {
-                if (lane == 0) atomicOr(&L.args[inst].ctl->status, ST_TMA);
+                if (lane == 0) atomicOr(&ctl_of(L, inst)->status, ST_TMA);
                 ended = true;  // the slot may still be read: leave without filling it
                 break;
             }
@@ -934,8 +1269,7 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
         int tries = 0;
         u64 t_wait = 0, last_done = ~0ull;
         for (;;) {
-            const InstArgs *A = L.args + inst;
-            InstCtl *C = A->ctl;
+            InstCtl *C = ctl_of(L, inst);
             u64 v = 0, lim = 0;
             u32 flags = 0;
             if (lane == 0) {
@@ -964,18 +1298,17 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
                 continue;
             }
             tries = 0;
-            bool all_done = true;
-            for (int q = lane; q < L.ninst; q += 32)
-                if (!(*(volatile u32 *)&L.args[q].ctl->flags & CTL_DONE)) all_done = false;
-            all_done = __all_sync(FULL, all_done);
-            if (all_done || !L.persist) {
+            if (!L.persist || launch_done(L, lane)) {
                 ended = true;
                 break;
             }
             // wait for a new plan (some instance's level is finishing); give up without progress
             u64 d = 0;
             if (lane == 0) {
-                for (int q = 0; q < L.ninst; ++q) d += ld_volatile(&L.args[q].ctl->done) + ld_volatile(&L.args[q].ctl->limit);
+                for (int q = 0; q < L.ninst; ++q) {
+                    InstCtl *Cq = ctl_of(L, q);
+                    d += ld_volatile(&Cq->done) + ld_volatile(&Cq->limit);
+                }
             }
             d = __shfl_sync(FULL, d, 0);
             const u64 now = globaltimer();
@@ -990,10 +1323,13 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
             __nanosleep(256);
         }
         if (ended) break;
-        const InstArgs *A = L.args + inst;
-        InstCtl *C = A->ctl;
-        // the plan's entry starts (per instance and sequence)
+        InstCtl *C = ctl_of(L, inst);
+        // the plan's arguments and entry starts (per instance and sequence)
         if (pc.inst != inst || pc.seq != (u32)tag) {
+            constexpr int AW = sizeof(InstArgs) / 8;
+            for (int w = lane; w < AW; w += 32)
+                reinterpret_cast<u64 *>(&pc.a)[w] = __ldcg(reinterpret_cast<const u64 *>(L.args + inst) + w);
+            __syncwarp();
             int nent = 0, rc = 1, ur = 1, cost = 0, chk = 0;
             long long pitems = 0;
             if (lane == 0) {
@@ -1005,7 +1341,7 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
                 pitems = __ldcg(&C->plan.items);
             }
             nent = __shfl_sync(FULL, nent, 0);
-            for (int e = lane; e < nent && e < ENTRY_CACHE; e += 32) pc.item0[e] = __ldcg(&A->entries[e].item0);
+            for (int e = lane; e < nent && e < ENTRY_CACHE; e += 32) pc.item0[e] = __ldcg(&pc.a.entries[e].item0);
             if (lane == 0) {
                 // rows of the finished levels were written through the generic proxy; the tile
                 // copies read them through the async proxy
@@ -1026,7 +1362,7 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
         int lo = 0, hi = pc.nentries - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            const long long m0 = mid < ENTRY_CACHE ? pc.item0[mid] : __ldcg(&A->entries[mid].item0);
+            const long long m0 = mid < ENTRY_CACHE ? pc.item0[mid] : __ldcg(&pc.a.entries[mid].item0);
             if (m0 <= item)
                 lo = mid;
             else
@@ -1034,7 +1370,7 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
         }
         if (pc.cur != lo) {
             constexpr int W = sizeof(Entry) / 8;
-            const u64 *src = reinterpret_cast<const u64 *>(A->entries + lo);
+            const u64 *src = reinterpret_cast<const u64 *>(pc.a.entries + lo);
             if (lane < W) reinterpret_cast<u64 *>(&pc.e)[lane] = __ldcg(src + lane);
             __syncwarp();
             if (lane == 0) pc.cur = lo;
@@ -1042,24 +1378,31 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
         }
         // skip rule: a find at or before this entry's block (or any find, find_first) in this level
         bool skip = false;
-        if (A->stop_at_found) {
+        if (pc.a.stop_at_found) {
             u64 fk = 0;
             if (lane == 0) fk = ld_volatile(&C->found_key);
             fk = __shfl_sync(FULL, fk, 0);
-            skip = fk != NO_FIND && (int)(fk >> 32) == pc.cost && (A->find_first || pc.e.pos >= (int)(u32)fk);
+            skip = fk != NO_FIND && (int)(fk >> 32) == pc.cost && (pc.a.find_first || pc.e.pos >= (int)(u32)fk);
+        }
+        {
+            constexpr int AW = sizeof(InstArgs) / 8;
+            for (int w = lane; w < AW; w += 32)
+                reinterpret_cast<u64 *>(&sl.args)[w] = reinterpret_cast<const u64 *>(&pc.a)[w];
+            __syncwarp();
         }
         if (lane == 0) {
-            const u32 bytes = fill_slot(sl, A, pc.e, item, L.tile, pc.rc, pc.ur, pc.cost, pc.check_only,
-                                        pc.plan_items, skip, A->pitch);
+            const u32 bytes = fill_slot(sl, inst, pc.e, item, L.tile, pc.rc, pc.ur, pc.cost, pc.check_only,
+                                        pc.plan_items, skip, pc.a.pitch);
             if (!skip) {
-                const u64 pitch = (u64)A->pitch;
+                const u64 pitch = (u64)pc.a.pitch;
                 const u64 rows_bytes = (u64)sl.nrows * pitch * 8;
-                if (rows_bytes > 0 && rows_bytes < (1ull << 31)) prefetch_l2(A->cache + (u64)sl.row0 * pitch, (u32)rows_bytes);
+                if (rows_bytes > 0 && rows_bytes < (1ull << 31))
+                    prefetch_l2(pc.a.cache + (u64)sl.row0 * pitch, (u32)rows_bytes);
             }
             if (bytes) {
                 fence_proxy_async();
                 mbar_expect_tx(&sl.full, bytes);
-                bulk_g2s(tiles + (u64)s * tile_words, A->cache + (u64)sl.l_first * A->pitch, bytes, &sl.full);
+                bulk_g2s(tiles + (u64)s * tile_words, pc.a.cache + (u64)sl.l_first * pc.a.pitch, bytes, &sl.full);
             } else {
                 mbar_arrive(&sl.full);
             }
@@ -1090,14 +1433,15 @@ __device__ void consumer(const Launch &L, unsigned char *smem, const u64 *tiles,
         if (lane == 0) ok = mbar_wait_for(&sl.full, (u32)((k / S) & 1), PIPE_WAIT_NS);
         ok = __shfl_sync(FULL, ok, 0);
         if (!ok) {
-            if (lane == 0) atomicOr(&L.args[0].ctl->status, ST_TMA);
+            if (lane == 0) atomicOr(&ctl_of(L, 0)->status, ST_TMA);
             return;
         }
         const int kind = *(volatile int *)&sl.kind;
         if (kind == 0) return;
-        const InstArgs &A = *sl.A;
+        const InstArgs &A = sl.args;
         InstCtl *C = A.ctl;
         const ulonglong2 *tile = reinterpret_cast<const ulonglong2 *>(tiles + (u64)s * tile_words);
+        int recycle = -1;  // a batch slot whose instance's search ended in this warp
         for (;;) {
             unsigned idx = 0;
             if (lane == 0) idx = atomicAdd(&sl.next_row, 1u);
@@ -1125,11 +1469,16 @@ __device__ void consumer(const Launch &L, unsigned char *smem, const u64 *tiles,
                     dd = atomicAdd(&C->done, 1ull);
                 }
                 dd = __shfl_sync(FULL, dd, 0);
-                if ((long long)dd + 1 == sl.plan_items) close_level(A, C, L.persist != 0, lane);
+                if ((long long)dd + 1 == sl.plan_items) {
+                    const bool ended = close_level(A, C, L.persist != 0, lane);
+                    if (ended && L.batch) recycle = sl.inst;
+                }
             }
         }
         if (lane == 0) mbar_arrive(&sl.empty);
         __syncwarp();
+        // the slot's next instance, outside the row loop (it takes a while and few values are live here)
+        if (recycle >= 0) next_instance<HK>(*L.batch, recycle, true, lane);
     }
 }
 
@@ -1160,6 +1509,13 @@ __global__ void __launch_bounds__(LEVEL_THREADS, 1) level_kernel(const Launch *_
         producer<TL>(L, smem, tiles, lane);
     else
         consumer<TL, HK>(L, smem, tiles, lane);
+}
+
+// A batch's first instances: block s sets slot s up (one warp per slot).
+template <int HK>
+__global__ void batch_start_kernel(BatchDev *__restrict__ B) {
+    if (threadIdx.x >= 32) return;
+    next_instance<HK>(*B, (int)blockIdx.x, false, threadIdx.x & 31);
 }
 
 // The first plan of each instance: the letters (cost c1, rows [0, nalpha)) form the level
@@ -1441,6 +1797,14 @@ int level_kernel_ctas_per_sm(int hk, size_t smem) {
 
 cudaError_t launch_first_plan(const InstArgs *d, int ninst, int open, cudaStream_t s) {
     first_plan_kernel<<<ninst, 32, 0, s>>>(d, open);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_start(BatchDev *d, int nslots, int hk, cudaStream_t s) {
+    if (hk == 1)
+        batch_start_kernel<1><<<nslots, 32, 0, s>>>(d);
+    else
+        batch_start_kernel<0><<<nslots, 32, 0, s>>>(d);
     return cudaGetLastError();
 }
 

@@ -160,9 +160,57 @@ struct InstArgs {
     const volatile u32 *cancel;  // host-mapped flag (or null): when set, the next level boundary ends the search
 };
 
+// ---- Batches: many independent instances drained by one launch.  The launch holds K
+// instance slots; each slot has its own buffers (InstArgs points into them).  When the search of
+// a slot's instance ends, the warp that closed its last level writes the instance's result and
+// sets the slot up with the next pending instance, so one launch learns the whole batch.
+constexpr int WALK_MAX = 256;  // entries of a result's formula tree (the reference's 200-node limit, the root)
+
+struct BatchIn {               // one instance of a batch: its traces in the batch's arrays
+    int npos, nneg, nalpha, pad;
+    long long steps0;          // first step of its traces in BatchDev::steps
+    long long offs0;           // first of its n + 1 offsets in BatchDev::offs (relative to steps0)
+    char alpha[32];            // sorted letters, NUL terminated
+};
+
+struct BatchOut {              // one instance's result
+    int status;                // ltlg_status; LTLG_NO_MEMORY: its slot's cache overflowed (learn it alone)
+    int cost;
+    u64 all_ltls;
+    u64 evaluated;
+    long long rows;
+    u64 found;                 // (1 << 63) | parents of the find (0: none or a letter)
+    int letter;                // index of the separating letter, or -1
+    int walk_count;            // entries of walk: (row, parents), breadth first, entry 0 the root
+    int walk_overflow;         // 1: the tree has more entries than the reference prints
+    u32 device_flags;
+    u64 ns;                    // device time from the slot's set-up to the result (globaltimer)
+    u64 walk[2 * WALK_MAX];
+};
+
+struct BatchDev {
+    const BatchIn *in;
+    const u32 *steps;
+    const int *offs;
+    BatchOut *out;
+    InstArgs *args;            // per slot (the slot's buffers and the learn's options; set-up fills the rest)
+    int *cur;                  // per slot: the instance it holds
+    u64 *t0;                   // per slot: globaltimer at its set-up
+    long long cache_words;     // per slot: language-cache words
+    long long max_rows;        // per slot: rows of parents (and keys)
+    int count;                 // instances
+    int nslots;
+    int max_pitch;
+    int pad;
+    unsigned long long next;   // next instance to take
+    int live;                  // slots holding an instance whose search runs
+    int pad2;
+};
+
 // A launch of the level kernel over one or more instances.
 struct Launch {
     const InstArgs *args;    // per instance
+    BatchDev *batch;         // or null: a batch drains its pending instances through the slots
     int ninst;
     int persist;             // 1: after a level, plan and run the next one in the same launch
     int tile;                // left rows staged per binary item (U: tile / 2 left rows, two candidates each)
@@ -210,6 +258,8 @@ constexpr int LEVEL_THREADS = 512;
 // launch (or a captured graph) stays valid while the arguments change between learns.
 cudaError_t launch_levels(const Launch &host_copy, const Launch *dev, int grid, int hash_kind, cudaStream_t s);
 cudaError_t launch_first_plan(const InstArgs *d, int ninst, int open, cudaStream_t s);
+// A batch's first instances: each slot takes pending instances until one needs levels.
+cudaError_t launch_batch_start(BatchDev *d, int nslots, int hash_kind, cudaStream_t s);
 cudaError_t launch_insert_letters(const InstArgs *d, int nalpha, int hash_kind, cudaStream_t s);
 cudaError_t launch_walk(const u64 *parents, int nalpha, u64 found, u64 *out, int cap, cudaStream_t s);
 // Plans level `cost` of the instance from its level starts (the levels below must be complete) and

@@ -251,6 +251,37 @@ def generate_hamming(seed: int, nprops: int, npos: int, nneg: int, lmin: int, lm
     raise RuntimeError("could not build a near-miss instance")
 
 
+def generate_near_miss(seed: int, nprops: int, npos: int, nneg: int, lmin: int, lmax: int,
+                       p_bit: float = 0.5, flips=(1, 3)) -> Instance:
+    """Near-miss instance without a hidden formula: npos random positives (Bernoulli(p_bit)
+    bits, lengths uniform lmin-lmax); each negative is a random positive with 1-3 random bits
+    flipped, and a flipped copy equal to a positive (or to an earlier negative) is drawn
+    again.  No separating formula of bounded size is planted."""
+    rng = np.random.default_rng(seed)
+    letters = "".join(sorted(DEFAULT_LETTERS[:nprops]))
+    lens, bits, _, _ = _draw(rng, npos, nprops, lmin, lmax, p_bit)
+    pos_l = [int(x) for x in lens]
+    pos_b = [bits[i] for i in range(npos)]
+    seen = {(ln, b[:ln].tobytes()) for ln, b in zip(pos_l, pos_b)}
+    neg_l, neg_b = [], []
+    for _ in range(1000 * max(1, nneg)):
+        if len(neg_l) == nneg:
+            break
+        src = int(rng.integers(npos))
+        ln = pos_l[src]
+        b = pos_b[src].copy()
+        for _k in range(int(rng.integers(flips[0], flips[1] + 1))):
+            b[int(rng.integers(ln)), int(rng.integers(nprops))] ^= True
+        key = (ln, b[:ln].tobytes())
+        if key in seen:
+            continue
+        seen.add(key)
+        neg_l.append(ln)
+        neg_b.append(b)
+    steps, offsets = _pack(letters, pos_l + neg_l, pos_b + neg_b)
+    return Instance(npos, len(neg_l), letters, steps, offsets, "")
+
+
 def hamming_neighbourhood(seed: int, nprops: int, length: int, delta: int = 1) -> Instance:
     """One random positive and every trace at Hamming distance exactly delta as negatives."""
     import itertools

@@ -7,7 +7,12 @@
   relaxed mode's completeness loss.
 * cfg4 — batched learning: 4096 independent instances (2-4 propositions, 8-256 positive and
   8-256 negative traces of length 4-40, Bernoulli(0.5), hidden formula of size 3-8, unit
-  costs) through the batch call, with the engine configuration picked by `autotune`.
+  costs) through the batch call (one persistent launch), with the configuration picked by
+  `autotune`.
+* cfg1 — the reference's own binary side by side: 2 propositions, 20 + 20 traces of length
+  8-16 (the committed cfg1 fixtures), this library's ltli6463 and the reference's ltli6463
+  built from its sources, same files and arguments, each one's printed Running Time, and the
+  same learn on a warm engine.
 
 Instances are seeded synthetic data of the shapes above (the reference ships none), made by
 the generator in child interpreters when `workers` > 1 (the generator is plain Python).
@@ -135,12 +140,12 @@ def cfg4_specs(count: int = 4096, seed: int = 0):
 
 
 AUTOTUNE_SPACE = [dict(left_tile=lt, right_chunk=rc, unary_rows=ur, slots_log2=sl, workers=w)
-                  for lt in (4, 8) for rc in (16, 64) for ur in (32, 64) for sl in (20, 22) for w in (8, 16)]
+                  for lt in (4, 8) for rc in (8, 32) for ur in (16, 64) for sl in (20, 22) for w in (48, 96)]
 
 
 def autotune(sample, space=AUTOTUNE_SPACE, cache_bytes=1 << 30, repeats=2, device=0, **opts):
     """Time the batch call on `sample` under every configuration of `space` (tile shapes,
-    item sizes, hash-set size = load factor, engines) and return (best, table)."""
+    item sizes, hash-set size = load factor, instance slots) and return (best, table)."""
     table = []
     for cfg in space:
         c = dict(cfg)
@@ -181,9 +186,55 @@ def run_cfg4(count=4096, seed=0, tune_sample=256, gen_workers=16, device=0) -> d
             "instances": count, "found": found, "seconds": el, "instances_per_s": count / el,
             "unique_cs_per_s": uniq / el, "min_cost": min(costs) if costs else None,
             "max_cost": max(costs) if costs else None,
-            "time_to_minimal_ms": {"mean": float(np.mean([r.seconds for r in res]) * 1e3),
-                                   "max": float(np.max([r.seconds for r in res]) * 1e3),
-                                   "note": "host wall time of each learn inside the concurrent batch"},
+            "time_to_minimal_ms": {"mean": float(np.mean([r.device_ms for r in res])),
+                                   "max": float(np.max([r.device_ms for r in res])),
+                                   "note": "device time of each instance from its slot's set-up to its result"},
+            "launches": "one batch-start launch and one level-kernel launch for the whole batch",
             "autotune": {"best": best, "sample": tune_sample, "configs": len(table),
                          "worst_seconds": max(t["seconds"] for t in table)},
             "generation_s": t_gen}
+
+
+# ---------------------------------------------------------------- cfg1
+CFG1_FILES = ("cfg1_s0.trace", "cfg1_s1.trace", "cfg1_s2.trace", "cfg1_s3.trace", "cfg1_deep.trace")
+
+
+def _parse_cli(out: str) -> dict:
+    lines = out.split("\n")
+    get = lambda key: next((ln.split(": ", 1)[1] for ln in lines if ln.startswith(key + ": ")), None)
+    t = get("Running Time")
+    formula = lines[-2][len('LTL: "'):-1] if len(lines) >= 2 and lines[-2].startswith("LTL: ") else None
+    return {"all_ltls": int(get("Number of All LTLs") or -1), "cost": int(get("Cost of Final LTL") or -1),
+            "seconds": float(t.split()[0]) if t else None, "formula": formula}
+
+
+def run_cfg1(reference_binary: str, fixtures_dir: str, max_cost: int = 6, rlx: int = 3, neg: int = 1,
+             timeout_s: float = 60.0) -> dict:
+    """This library's ltli6463 and the reference's, on the same cfg1 files and arguments (unit
+    costs); each one's printed Running Time (both include their process's CUDA context and
+    device allocations) and the time of the same learn on a warm in-process engine."""
+    rows = []
+    have_ref = os.path.exists(reference_binary)
+    with api.Engine(slots_log2=22, cache_bytes=2 << 30, max_rows=4 << 20) as eng:
+        for name in CFG1_FILES:
+            path = os.path.join(fixtures_dir, name)
+            args = [path] + ["1"] * 8 + [str(max_cost), str(rlx), str(neg)]
+            mine = _parse_cli(subprocess.run([api.CLI_PATH] + args, capture_output=True, text=True,
+                                             timeout=timeout_s).stdout)
+            ref = None
+            if have_ref:
+                ref = _parse_cli(subprocess.run([reference_binary] + args, capture_output=True, text=True,
+                                                timeout=timeout_s).stdout)
+            inst = gen.from_scarlet_text(open(path).read())
+            eng.learn(inst, max_cost=max_cost, neg_type=neg)
+            warm = eng.learn(inst, max_cost=max_cost, neg_type=neg)
+            rows.append({"file": name, "cost": mine["cost"], "reference_cost": ref["cost"] if ref else None,
+                         "all_ltls": mine["all_ltls"], "reference_all_ltls": ref["all_ltls"] if ref else None,
+                         "cli_s": mine["seconds"], "reference_s": ref["seconds"] if ref else None,
+                         "warm_engine_ms": warm.seconds * 1e3, "warm_engine_device_ms": warm.device_ms})
+    out = {"workload": f"cfg1: 2 props, 20+20 traces, len U[8,16] (the committed cfg1 fixtures), unit costs, "
+                       f"maxCost {max_cost}, RlxUnqChkTyp {rlx}, NegType {neg}",
+           "files": rows}
+    if not have_ref:
+        out["reference"] = "unavailable: the reference binary is not built (oracle/Makefile, target ref)"
+    return out

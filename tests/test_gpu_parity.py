@@ -228,6 +228,20 @@ def test_gpu_matches_reference_outputs(engine, run):
         assert O.formula_cost(res.formula, run["costs"]) == fin["cost"]
 
 
+@pytest.mark.parametrize("run", _golden_exact_runs(), ids=lambda r: r["id"])
+def test_fused_count_matches_reference_outputs(engine, run):
+    """The default (fused) schedule against the reference binary's final lines: the same cost
+    and the same "Number of All LTLs", which counts a found level through the first block of
+    the reference's order that holds an accepting candidate (ltli6463.cu:1232-1234), whichever
+    warp finds first on the device."""
+    inst = load_fixture(run["file"])
+    fin = run["final"]
+    for _ in range(3):
+        res = engine.learn(inst, costs=run["costs"], max_cost=run["max_cost"], neg_type=run["neg"],
+                           limit_traces=True)
+        assert (res.cost, res.all_ltls) == (fin["cost"], fin["all_ltls"])
+
+
 def test_batch_learn_matches_single_engine():
     insts = [gen.generate(2000 + s, 3, 40, 40, 5, 20, 0.5, 6) for s in range(16)]
     with api.Batch(workers=4, slots_log2=22, cache_bytes=1 << 30, max_rows=1 << 20) as pool:

@@ -156,3 +156,25 @@ def test_publication_wait_runs_out():
         res = e.learn(inst, max_cost=3, stop_at_found=False, neg_type=1)
         assert res.status == api.DEVICE_WAIT and res.device_flags & 2
         assert_level_sets(e, inst, 4)
+
+
+def test_costs_and_splits_beyond_old_caps():
+    """Expensive operators (costs of 100, maxCost 5000) find at cost 900, past the 511 level
+    starts the device once kept; cheap letters with uneven operator costs give levels with more
+    than 64 splits per operator (the reference has no split cap, ltli6463.cu:1245).  Cost and
+    candidate count equal the oracle's, and every level's set of CSs up to cost 600."""
+    inst = load_fixture("ham1_len3.trace")
+    with api.Engine(slots_log2=22, cache_bytes=1 << 30, max_rows=1 << 20) as e:
+        for costs in ([100] * 8, [100, 100, 150, 150, 100, 200, 200, 300]):
+            res = e.learn(inst, costs=costs, max_cost=5000, neg_type=1)
+            ref = O.learn(inst, costs=costs, max_cost=5000, neg_type=1, keep_rows=False)
+            assert res.status == api.FOUND and ref.status == O.FOUND and res.cost > 511
+            assert (res.cost, res.all_ltls) == (ref.cost, ref.all_ltls)
+            assert O.separates(res.formula, inst) and O.formula_cost(res.formula, costs) == res.cost
+        costs = [1, 37, 41, 43, 29, 53, 59, 61]
+        res, ref = assert_level_sets(e, inst, 600, costs=costs)
+    ls = [ref.level_start[k] for k in range(602)]
+    nonempty = {k for k in range(601) if ls[k + 1] > ls[k]}
+    splits = max(sum(1 for i in nonempty if 2 * i <= c - cop and (c - i - cop) in nonempty)
+                 for c in range(601) for cop in (costs[2], costs[3], costs[7]))
+    assert splits > 64, splits

@@ -49,6 +49,7 @@ def test_noalloc_matches_learn_found(name, make):
         rc, formula, cost, all_ltls = noalloc(inst, neg_type=1)
         assert rc == want.status == api.FOUND
         assert cost == want.cost
+        assert all_ltls == want.all_ltls  # the reference's count: blocks in order up to the first find
         assert O.separates(formula, inst), formula
         assert O.formula_cost(formula) == cost
 

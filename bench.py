@@ -370,7 +370,7 @@ def run_ours(a):
 
     step_ms, kern_ms, launches = [], [], 0
     uniq_e2e = cand_e2e = uniq_seq = cand_seq = 0
-    level_launches = 0  # level-kernel launches of the one-at-a-time pass
+    level_launches = 0  # level-kernel launches of the one-at-a-time pass (one per learn that ran levels)
     ttm, costs = [], []
     h2d = d2h = 0
     with Clocks(local, enabled=not a.no_clocks) as clk:
@@ -386,11 +386,11 @@ def run_ours(a):
             torch.cuda.synchronize()
             barrier()
             step_ms.append(e0.elapsed_time(e1))
+            launches += 2 if pool else sum(r.launches for r in res)  # the batch call: its start and level launches
             for inst, r in zip(batch, res):
                 assert r.status == api.FOUND or a.no_stop, (r.status, r.formula)
                 uniq_e2e += r.rows - len(inst.alphabet)
                 cand_e2e += r.evaluated - len(inst.alphabet)
-                launches += r.launches
                 ttm.append(r.device_ms)
                 costs.append(r.cost)
                 h2d += len(inst.alphabet) * inst.n * 8 + inst.n * 12  # letter CSs + word metadata
@@ -402,7 +402,7 @@ def run_ours(a):
             for inst, r in zip(batch, seq):
                 uniq_seq += r.rows - len(inst.alphabet)
                 cand_seq += r.evaluated - len(inst.alphabet)
-                level_launches += len(r.levels)
+                level_launches += 1 if r.levels else 0  # one persistent level-kernel launch per learn
     clocks = clk.summary()
     K = a.steps
     step_t = sum(step_ms) / 1e3
@@ -454,12 +454,13 @@ def run_ours(a):
             line["learned_order"] = learned_order_report(ekw)
         if ws == 1 and not a.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(batch, a.cpu_sample_s)
-        if ws == 1 and not a.no_extras:
-            line.update(extras(local, a.time_limit))
-        print(json.dumps(line), flush=True)
     if pool:
         pool.close()
     eng.close()
+    if rank == 0:
+        if ws == 1 and not a.no_extras:  # after the timed buffers are released: cfg3 wants most of HBM
+            line.update(extras(local, a.time_limit))
+        print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as D
         D.destroy_process_group()

@@ -100,9 +100,10 @@ typedef struct ltlg_engine_config {
                                   polls about 128 ns apart; a wait that runs out ends the learn with
                                   LTLG_DEVICE_WAIT.  0 = 2^22 (about half a second) */
     int32_t pad_;
-    int64_t small_level;       /* levels with fewer candidates are cut into work items of small_rows
-                                  rows; larger levels use right_chunk / unary_rows.  0 = the size
-                                  below which large items would give fewer than four per CTA */
+    int64_t small_level;       /* levels with fewer candidates are cut into work items of about
+                                  rows / (2 x CTAs x item slots) rows each (at least small_rows, at
+                                  most right_chunk / unary_rows); larger levels use right_chunk /
+                                  unary_rows.  0 = every level is sized that way */
 } ltlg_engine_config;
 
 typedef struct ltlg_options {

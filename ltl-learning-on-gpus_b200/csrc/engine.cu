@@ -612,13 +612,13 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     A.small_rows = std::max(1, e->cfg.small_rows);
     A.tile = tile;
     A.gen = e->gen;
-    // small levels: where big items would give fewer than four per CTA
-    A.small_level = e->cfg.small_level > 0 ? e->cfg.small_level
-                                           : (long long)e->grid * 4 * tile * std::max(1, e->cfg.right_chunk);
+    // by default every level sizes its items from its own size (up to the big sizes)
+    A.small_level = e->cfg.small_level > 0 ? e->cfg.small_level : LLONG_MAX / 2;
     A.wait_spins = e->cfg.wait_spins > 0 ? e->cfg.wait_spins : (1ll << 22);
     A.cap_rows = cap_rows;
     A.cap_entries = cap_entries;
     A.learn_min_items = (long long)e->grid * stages;
+    A.item_target = (long long)e->grid * stages * 2;
     A.slot_mask = e->nslots - 1;
     A.cache = (u64 *)e->cache.p;
     A.parents = (u64 *)e->parents.p;
@@ -1279,11 +1279,11 @@ LTLG_API int ltlg_batch_learn(ltlg_batch *b, const ltlg_traces *traces, int32_t 
                 A.small_rows = std::max(1, b->cfg.small_rows);
                 A.tile = tile;
                 A.gen = b->gen[s2];
-                A.small_level = b->cfg.small_level > 0 ? b->cfg.small_level
-                                                       : (long long)grid * 4 * tile * std::max(1, b->cfg.right_chunk);
+                A.small_level = b->cfg.small_level > 0 ? b->cfg.small_level : LLONG_MAX / 2;
                 A.wait_spins = b->cfg.wait_spins > 0 ? b->cfg.wait_spins : (1ll << 22);
                 A.cap_entries = cap_entries;
                 A.learn_min_items = (long long)grid * stages;
+                A.item_target = (long long)grid * stages * 2;
                 A.slot_mask = nslots - 1;
                 A.cache = (u64 *)b->cache.p + (size_t)s2 * cache_words;
                 A.parents = (u64 *)b->parents.p + (size_t)s2 * max_rows;

@@ -532,8 +532,10 @@ __device__ __forceinline__ void store_entry(Entry *dst, const Entry &e) {
 // The binary blocks of operator op (cost cop) of level c, in the reference's split order
 // (i = c1 .. (c - cop) / 2 over non-empty levels i and j = c - i - cop): written as entries
 // from queue index *eidx and positions from *pos.  Returns the candidates of this lane's blocks.
-__device__ u64 plan_binary(const InstArgs &A, int c, int op, int ne_count, int &pos, int &eidx, int lane) {
+__device__ u64 plan_binary(const InstArgs &A, int c, int op, int ne_count, int &pos, int &eidx, u64 &units,
+                           int lane) {
     const int cop = A.cf[op + 1], c1 = A.cf[0];
+    const int tl = op == OP_U ? max(1, A.tile / 2) : A.tile;
     u64 cand = 0;
     if (c - cop < 2 * c1) return 0;
     for (int base = 0; base < ne_count; base += 32) {
@@ -562,6 +564,7 @@ __device__ u64 plan_binary(const InstArgs &A, int c, int op, int ne_count, int &
             e.r1 = hj;
             e.cand = (u64)(op == OP_U ? 2 : 1) * (u64)(hi_ - li) * (u64)(hj - lj);
             cand += e.cand;
+            units += (u64)((hi_ - li + tl - 1) / tl) * (u64)(hj - lj);
             store_entry(A.entries + eidx + rank, e);
         }
         pos += __popc(m);
@@ -613,11 +616,12 @@ __device__ void plan_level(const InstArgs &A, InstCtl *C, int c, int lane) {
     int pos = 0, eidx = nu;
     int upos[4] = {POS_NONE, POS_NONE, POS_NONE, POS_NONE};
     if (um & 1u) upos[0] = pos++;
-    u64 cand = plan_binary(A, c, OP_AND, ne_count, pos, eidx, lane);
-    cand += plan_binary(A, c, OP_OR, ne_count, pos, eidx, lane);
+    u64 units_b = 0, units_u = 0;  // binary: (left tile, right row) pairs; unary: source rows
+    u64 cand = plan_binary(A, c, OP_AND, ne_count, pos, eidx, units_b, lane);
+    cand += plan_binary(A, c, OP_OR, ne_count, pos, eidx, units_b, lane);
     for (int j = 1; j < 4; ++j)
         if ((um >> j) & 1u) upos[j] = pos++;
-    cand += plan_binary(A, c, OP_U, ne_count, pos, eidx, lane);
+    cand += plan_binary(A, c, OP_U, ne_count, pos, eidx, units_b, lane);
     if (lane == 0) {
         for (int g = 0; g < nu; ++g) {
             Entry e{};
@@ -635,18 +639,29 @@ __device__ void plan_level(const InstArgs &A, InstCtl *C, int c, int lane) {
                 e.cand += (u64)(hi4[j] - lo4[j]);
             }
             cand += e.cand;
+            units_u += (u64)(e.r1 - e.r0);
             store_entry(A.entries + g, e);
         }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cand += __shfl_xor_sync(FULL, cand, o);
+    for (int o = 16; o > 0; o >>= 1) {
+        cand += __shfl_xor_sync(FULL, cand, o);
+        units_b += __shfl_xor_sync(FULL, units_b, o);
+        units_u += __shfl_xor_sync(FULL, units_u, o);
+    }
     const int nent = eidx, nblocks = pos;
     __threadfence_block();
-    // Item sizes: a level with fewer candidates than small_level is cut into small items
-    // (small_rows rows each), so every SM takes part; larger levels use the big sizes.
+    // Item sizes: a level with fewer candidates than small_level is cut into items of about
+    // units / item_target rows (at least small_rows), so every SM's slots take part and each
+    // claim brings a few rows; larger levels use the big sizes.
     const bool small = (long long)cand < A.small_level;
-    const int rc = max(1, small ? A.small_rows : A.right_chunk_big);
-    const int ur = max(1, small ? A.small_rows : A.unary_rows_big);
+    const long long tgt = max(1ll, A.item_target);
+    const int rc = small ? (int)max((long long)max(1, A.small_rows),
+                                    min((long long)A.right_chunk_big, ((long long)units_b + tgt - 1) / tgt))
+                         : max(1, A.right_chunk_big);
+    const int ur = small ? (int)max((long long)max(1, A.small_rows),
+                                    min((long long)A.unary_rows_big, ((long long)units_u + tgt - 1) / tgt))
+                         : max(1, A.unary_rows_big);
     long long items = 0;
     for (int base = 0; base < nent; base += 32) {
         const int e = base + lane;
@@ -1249,7 +1264,7 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
     __syncwarp();
     int inst = (int)(blockIdx.x % (unsigned)L.ninst);
     u64 k = 0;
-    bool ended = false;
+    bool ended = false, optimistic = false;
     while (!ended) {
         const int s = (int)(k % (u64)S);
         Slot &sl = *slot_at(smem, s);
@@ -1263,35 +1278,45 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
                 break;
             }
         }
-        // claim an item from some instance
+        // claim an item from some instance.  After a successful claim the next one is
+        // optimistic: the limit, the find key and the claim are issued together (one round
+        // trip); after a failed one the producer looks before it takes, so idle polls do not
+        // advance the counter.
         long long item = -1;
-        u64 tag = 0;
+        u64 tag = 0, fk = NO_FIND;
         int tries = 0;
         u64 t_wait = 0, last_done = ~0ull;
         for (;;) {
             InstCtl *C = ctl_of(L, inst);
-            u64 v = 0, lim = 0;
-            u32 flags = 0;
+            u64 v = 0, lim = 0, f = NO_FIND;
             if (lane == 0) {
-                // look before taking, so idle polls do not advance the counter
-                lim = ld_acquire(&C->limit);
-                const u64 cur = ld_volatile(&C->claimed);
-                v = cur;
-                if ((cur >> SEQ_SHIFT) == (lim >> SEQ_SHIFT) && cur < lim) {
+                if (optimistic) {
+                    lim = ld_volatile(&C->limit);
+                    f = ld_volatile(&C->found_key);
                     v = atomicAdd(&C->claimed, 1ull);
-                    lim = ld_acquire(&C->limit);
+                    if ((v >> SEQ_SHIFT) != (lim >> SEQ_SHIFT)) lim = ld_volatile(&C->limit);  // a newer plan
+                } else {
+                    lim = ld_volatile(&C->limit);
+                    const u64 cur = ld_volatile(&C->claimed);
+                    v = cur;
+                    if ((cur >> SEQ_SHIFT) == (lim >> SEQ_SHIFT) && cur < lim) {
+                        f = ld_volatile(&C->found_key);
+                        v = atomicAdd(&C->claimed, 1ull);
+                        lim = ld_volatile(&C->limit);
+                    }
                 }
-                flags = *(volatile u32 *)&C->flags;
             }
             v = __shfl_sync(FULL, v, 0);
             lim = __shfl_sync(FULL, lim, 0);
-            flags = __shfl_sync(FULL, flags, 0);
-            (void)flags;
+            f = __shfl_sync(FULL, f, 0);
             if ((v >> SEQ_SHIFT) == (lim >> SEQ_SHIFT) && v < lim) {
                 item = (long long)(v & ITEM_MASK);
                 tag = v >> SEQ_SHIFT;
+                fk = f;
+                optimistic = true;
                 break;
             }
+            optimistic = false;
             // nothing to take from this instance now
             if (++tries < L.ninst) {
                 inst = (inst + 1) % L.ninst;
@@ -1326,6 +1351,7 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
         InstCtl *C = ctl_of(L, inst);
         // the plan's arguments and entry starts (per instance and sequence)
         if (pc.inst != inst || pc.seq != (u32)tag) {
+            __threadfence();  // the new plan was published before the claim counter this claim read
             constexpr int AW = sizeof(InstArgs) / 8;
             for (int w = lane; w < AW; w += 32)
                 reinterpret_cast<u64 *>(&pc.a)[w] = __ldcg(reinterpret_cast<const u64 *>(L.args + inst) + w);
@@ -1377,13 +1403,8 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
             __syncwarp();
         }
         // skip rule: a find at or before this entry's block (or any find, find_first) in this level
-        bool skip = false;
-        if (pc.a.stop_at_found) {
-            u64 fk = 0;
-            if (lane == 0) fk = ld_volatile(&C->found_key);
-            fk = __shfl_sync(FULL, fk, 0);
-            skip = fk != NO_FIND && (int)(fk >> 32) == pc.cost && (pc.a.find_first || pc.e.pos >= (int)(u32)fk);
-        }
+        const bool skip = pc.a.stop_at_found && fk != NO_FIND && (int)(fk >> 32) == pc.cost &&
+                          (pc.a.find_first || pc.e.pos >= (int)(u32)fk);
         {
             constexpr int AW = sizeof(InstArgs) / 8;
             for (int w = lane; w < AW; w += 32)

@@ -136,11 +136,12 @@ struct InstArgs {
     int tile;            // left rows staged per binary item (U: tile / 2 left rows)
     u32 gen;             // hash-set generation (1..255)
     int pad_;
-    long long small_level;  // levels with fewer candidates use small items
+    long long small_level;  // levels with fewer candidates size their items from the level (item_target)
     long long wait_spins;   // polls (~128 ns apart) before a wait for a slot publication gives up
     long long cap_rows;
     long long cap_entries;  // capacity of entries / found_par (entries holds twice that: the second half is scratch)
     long long learn_min_items;  // PLAN_LEARNED: plans of at most this many items keep the plain order
+    long long item_target;  // small levels are cut into about this many items
     u64 slot_mask;
     u64 *cache;
     u64 *parents;

@@ -275,8 +275,9 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     A.small_rows = 1;
     A.tile = tile;
     A.gen = 1;  // the slots were just cleared
-    A.small_level = (long long)grid * 4 * tile * 64;
+    A.small_level = LLONG_MAX / 2;
     A.wait_spins = 1ll << 22;
+    A.item_target = (long long)grid * stages * 2;
     A.cap_rows = cap;
     A.cap_entries = cap_entries;
     A.slot_mask = nslots - 1;

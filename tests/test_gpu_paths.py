@@ -43,10 +43,9 @@ def engine():
 
 @pytest.mark.parametrize("right_chunk,unary_rows", [(16, 32), (7, 5)])
 def test_large_level_items_thousand_traces(right_chunk, unary_rows):
-    """The 500 + 500-trace shape with every level cut into large-level items (a warp takes
-    several right rows of a tile, unary items of several source rows), through cost 7, where
-    the default threshold keeps these levels on one row per warp.  Odd sizes leave ragged
-    item ends."""
+    """The 500 + 500-trace shape with every level cut into the large items (right_chunk right
+    rows per tile, unary_rows source rows), through cost 7, where the default sizing gives
+    these levels smaller items.  Odd sizes leave ragged item ends."""
     inst = gen.generate(2, 3, 500, 500, 16, 32, 0.5, 9)
     with api.Engine(slots_log2=24, cache_bytes=4 << 30, max_rows=8 << 20, small_level=1, right_chunk=right_chunk,
                     unary_rows=unary_rows) as e:

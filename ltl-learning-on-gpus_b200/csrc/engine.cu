@@ -358,7 +358,9 @@ namespace {
 // time limit (the planner ends the search at the next level boundary once the cancel flag is set).
 cudaError_t run_levels(ltlg_engine *e, bool persist, int grid, double t0, double time_limit_s, LoopOut &o) {
     Launch *hl = (Launch *)e->h_launch.p;
+    memset(hl, 0, sizeof(Launch));  // no batch: one instance
     hl->args = (const InstArgs *)e->args.p;
+    hl->batch = nullptr;
     hl->ninst = 1;
     hl->persist = persist ? 1 : 0;
     hl->tile = e->tile;

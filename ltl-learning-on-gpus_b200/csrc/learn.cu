@@ -311,16 +311,18 @@ __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost,
             if (vm) {
                 u32 diff = 0;
                 const u32 myv = (u32)vrow;
+                const ulonglong2 *vr[NC];
+#pragma unroll
+                for (int t = 0; t < NC; ++t)
+                    vr[t] = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)__shfl_sync(FULL, myv, t) * pitch);
 #pragma unroll 4
                 for (int c = lane; c < nch; c += 32) {
                     const ulonglong2 p = g.pre(c);
 #pragma unroll
                     for (int t = 0; t < NC; ++t) {
                         if ((vm >> t) & 1u) {
-                            const u32 vr = __shfl_sync(FULL, myv, t);
                             const ulonglong2 a = g.word(t, c, p);
-                            const ulonglong2 b =
-                                __ldcg(reinterpret_cast<const ulonglong2 *>(A.cache + (u64)vr * pitch) + c);
+                            const ulonglong2 b = __ldcg(vr[t] + c);
                             diff |= (u32)((a.x != b.x) | (a.y != b.y)) << t;
                         }
                     }

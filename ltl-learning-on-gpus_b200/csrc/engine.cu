@@ -93,7 +93,7 @@ struct ltlg_engine {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
     // device buffers of the instance
-    DevBuf cache, parents, keys, slots, wmeta, kmeta, ls, ne, lcands, lns, lstats, entries, fpar;
+    DevBuf cache, parents, keys, prio, slots, wmeta, kmeta, ls, ne, lcands, lns, lstats, entries, fpar;
     DevBuf ctl, args, launch, walk, snaps, scorer, scorer_params;
     // pinned host copies
     DevBuf h_ctl, h_args, h_launch, h_walk, h_stage, h_ls, h_lcands, h_lns, h_ne, h_snaps, h_win, h_entries, h_fpar,
@@ -328,7 +328,7 @@ LTLG_API void ltlg_engine_destroy(ltlg_engine *e) {
     if (!e) return;
     cudaSetDevice(e->cfg.device);
     if (e->stream) cudaStreamSynchronize(e->stream);
-    for (DevBuf *b : {&e->cache, &e->parents, &e->keys, &e->slots, &e->wmeta, &e->kmeta, &e->ls, &e->ne, &e->lcands,
+    for (DevBuf *b : {&e->cache, &e->parents, &e->keys, &e->prio, &e->slots, &e->wmeta, &e->kmeta, &e->ls, &e->ne, &e->lcands,
                       &e->lns, &e->lstats, &e->entries, &e->fpar, &e->ctl, &e->args, &e->launch, &e->walk, &e->snaps,
                       &e->scorer, &e->scorer_params})
         if (b->p) cudaFree(b->p);
@@ -543,6 +543,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     if ((err = ensure(e->parents, (size_t)cap_rows * 8)) != cudaSuccess) return fail_cuda(e, err, res);
     if (opt->key_mode != LTLG_KEY_EXACT && (err = ensure(e->keys, (size_t)cap_rows * 16)) != cudaSuccess)
         return fail_cuda(e, err, res);
+    if (ref_keys && (err = ensure(e->prio, (size_t)cap_rows * 8)) != cudaSuccess) return fail_cuda(e, err, res);
     if ((err = ensure(e->wmeta, (size_t)pitch * 8)) != cudaSuccess) return fail_cuda(e, err, res);
     if ((err = ensure(e->kmeta, (size_t)pitch * 4)) != cudaSuccess) return fail_cuda(e, err, res);
     if ((err = ensure(e->ls, (size_t)ncost * 8)) != cudaSuccess) return fail_cuda(e, err, res);
@@ -625,6 +626,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     A.cache = (u64 *)e->cache.p;
     A.parents = (u64 *)e->parents.p;
     A.keys = opt->key_mode != LTLG_KEY_EXACT ? (u64 *)e->keys.p : nullptr;
+    A.prio = ref_keys ? (u64 *)e->prio.p : nullptr;
     A.slots = (u64 *)e->slots.p;
     A.wmeta = (const u64 *)e->wmeta.p;
     A.kmeta = (const u32 *)e->kmeta.p;

@@ -56,6 +56,7 @@ struct Slot {
     u64 empty;                // mbarrier: every consumer left the slot
     long long row0;           // binary: first right row; unary: first source row
     long long l_first;        // binary: first left row of the tile
+    long long e_l0, e_r0, e_R;  // the entry's first left row, first right (source) row, right rows
     long long plan_items;     // items of the plan: the item done that brings `done` to it ends the level
     unsigned next_row;        // consumers take rows here
     unsigned rows_done;
@@ -191,9 +192,39 @@ __device__ __forceinline__ void count_row_stats(u64 *cnt, bool stored, u32 pmiss
 // claimed rows, verifying fingerprint matches) is one chunk-major sweep over all the
 // candidates concerned, so their loads are in flight together.  Claims are written and
 // published before any lane waits on another warp's publication, so waits cannot cycle.
+// The reference's relaxed keys keep, of the CSs that share a key in a level, the one its
+// threads insert first: blocks run in order and, within a block, thread order (the oracle's
+// tid order, which the reference's recorded runs follow).  Here the row of a key records the
+// priority (block position << 40 | the reference's thread index, U's "l U r" before "r U l")
+// of the candidate it holds; a candidate of the same level with the same key and a lower
+// priority takes the row over: it locks the priority word (bit 0), rewrites the row and its
+// parent, and publishes its priority.  Rows of lower levels are never taken over.  One lane,
+// bounded waits.
+template <class Gen>
+__device__ void take_over(const InstArgs &A, InstCtl *C, const Gen &g, int t, u64 row, u64 prio, u64 parent) {
+    u64 *pw = A.prio + row;
+    const int nch = A.pitch >> 1;
+    for (long long spin = 0; spin < A.wait_spins; ++spin) {
+        const u64 v = ld_acquire(pw);
+        if ((v >> 1) <= prio) return;  // the row holds an earlier candidate (or this one)
+        if (v & 1ull) {                // another take-over is writing the row
+            __nanosleep(128);
+            continue;
+        }
+        if (atomicCAS(pw, v, (prio << 1) | 1ull) != v) continue;
+        ulonglong2 *dst = reinterpret_cast<ulonglong2 *>(A.cache + row * (u64)A.pitch);
+        for (int c = 0; c < nch; ++c) dst[c] = g.word(t, c, g.pre(c));
+        A.parents[row] = parent;
+        __threadfence();
+        st_release(pw, prio << 1);
+        return;
+    }
+    atomicOr(&C->status, ST_WAIT);
+}
+
 template <int NC, class Gen>
 __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost, const Gen &g, u64 fp, bool active,
-                                        u64 parent, u64 kh, u64 kl, u32 anyp, u32 anyn, int lane) {
+                                        u64 parent, u64 kh, u64 kl, u64 prio, u32 anyp, u32 anyn, int lane) {
     int state = active ? S_PROBE : S_DONE;
     const u64 tagbits = (fp >> 40) << 40;
     const u64 genbits = (u64)A.gen << 32;
@@ -274,6 +305,7 @@ __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost,
                     A.keys[2 * myrow] = kh;
                     A.keys[2 * myrow + 1] = kl;
                 }
+                if (A.prio) A.prio[myrow] = prio << 1;
             }
             __threadfence();
             __syncwarp();
@@ -340,6 +372,7 @@ __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost,
         } else if (state == S_VERIFY) {
             const u64 eh = __ldcg(A.keys + 2 * vrow), el = __ldcg(A.keys + 2 * vrow + 1);
             if (eh == kh && el == kl) {
+                if (A.prio && vrow >= __ldcg(A.ls + cost)) take_over(A, C, g, lane, (u64)vrow, prio, parent);
                 state = S_DONE;
             } else {
                 state = S_PROBE;
@@ -351,9 +384,9 @@ __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost,
 
 // Fingerprints, acceptance, the find record, uniqueness for NC candidates of one warp.
 // pos_of(t): block position of candidate t (the find record is per block).
-template <int NC, class Gen, class ParentOf, class PosOf>
+template <int NC, class Gen, class ParentOf, class PosOf, class TidOf>
 __device__ __forceinline__ void finish(const InstArgs &A, InstCtl *C, Slot &sl, const Gen &g, u64 (&h)[NC], u32 bp,
-                                       u32 bn, u32 valid, ParentOf parent_of, PosOf pos_of, int lane) {
+                                       u32 bn, u32 valid, ParentOf parent_of, PosOf pos_of, TidOf tid_of, int lane) {
     const u64 sum = reduce_to_lane<NC>(h, lane);
     const u32 anyp = __reduce_or_sync(FULL, bp), anyn = __reduce_or_sync(FULL, bn);
     const u32 acc = ~(anyp | anyn) & valid;
@@ -388,7 +421,8 @@ __device__ __forceinline__ void finish(const InstArgs &A, InstCtl *C, Slot &sl, 
         }
         fp = fmix64(kh ^ fmix64(kl + 0x5ad0dedull));
     }
-    resolve<NC>(A, C, cost, g, fp, (valid >> lane) & 1u, myparent, kh, kl, anyp, anyn, lane);
+    const u64 prio = A.prio && ((valid >> lane) & 1u) ? ((u64)(u32)pos_of(lane) << 40) | tid_of(lane) : 0ull;
+    resolve<NC>(A, C, cost, g, fp, (valid >> lane) & 1u, myparent, kh, kl, prio, anyp, anyn, lane);
 }
 
 // ---------------------------------------------------------------- rows
@@ -459,7 +493,13 @@ __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &
                    }
                    return pack_parent(rop, (u64)(l_first + t), (u64)r);
                },
-               [&](int) { return sl.pos; }, lane);
+               [&](int) { return sl.pos; },
+               [&](int t) -> u64 {  // the reference's thread index: (l - l0) * R + (r - r0); U: both orders
+                   const u64 l = (u64)(l_first + (OPC == OP_U ? (t >> 1) : t));
+                   const u64 tid = (l - (u64)sl.e_l0) * (u64)sl.e_R + ((u64)r - (u64)sl.e_r0);
+                   return OPC == OP_U ? 2 * tid + (u64)(t & 1) : tid;
+               },
+               lane);
     if (lane == 0) atomicAdd(&sl.evals, (unsigned)cnt);
 }
 
@@ -507,7 +547,7 @@ __device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &s
     const UnGen g{src, meta};
     finish<NC>(A, C, sl, g, h, bp, bn, valid,
                [&](int t) { return pack_parent(unary_slot_op(t & 3), (u64)s, 0); },
-               [&](int t) { return sl.upos[t & 3]; }, lane);
+               [&](int t) { return sl.upos[t & 3]; }, [&](int) -> u64 { return (u64)(s - sl.e_r0); }, lane);
     if (lane == 0) atomicAdd(&sl.evals, (unsigned)__popc(valid));
 }
 
@@ -1205,6 +1245,9 @@ __device__ __forceinline__ u32 fill_slot(Slot &sl, int inst, const Entry &e, lon
     sl.rows_done = 0;
     sl.evals = 0;
     sl.stop = skip ? 1 : 0;
+    sl.e_l0 = e.l0;
+    sl.e_r0 = e.r0;
+    sl.e_R = e.r1 - e.r0;
     if (e.kind == ENT_UNARY) {
         sl.op = e.opmask;
         sl.row0 = e.r0 + local * ur;

@@ -146,6 +146,7 @@ struct InstArgs {
     u64 *cache;
     u64 *parents;
     u64 *keys;           // 2 words per row for KEY_REF / KEY_HASH64, else null
+    u64 *prio;           // KEY_REF: per row, the priority of the candidate it holds << 1 | lock (else null)
     u64 *slots;
     const u64 *wmeta;    // per word: length mask | (positive << 63); 0 for padding
     const u32 *kmeta;    // KEY_REF: per word start | count << 16 | step << 24

@@ -85,15 +85,21 @@ def _relaxed_golden_runs():
 
 @pytest.mark.parametrize("run", _relaxed_golden_runs(), ids=lambda r: r["id"])
 def test_reference_keys_match_reference_runs(engine, run):
-    """The reference's relaxed keys (types 1/2/3, lenSum > 126) on the device against the
-    reference binary's own progress lines: cost 2 is built from letters only and matches
-    exactly; after it, which of two CSs sharing a key is kept is a race in the reference, and
-    the stored counts may drift by at most 1%.  The final cost is the reference's."""
+    """The reference's relaxed keys (types 1/2/3, lenSum > 126) on the device.  Of the CSs that
+    share a key in a level, the device keeps the one the reference's threads insert first
+    (blocks in order, thread order inside a block), as the oracle does: per-level sets of rows
+    and the per-block progress lines equal the oracle's exactly, in both schedules.  Against the
+    reference binary's own progress lines the rule of the oracle's pinning applies: cost 2 is
+    built from letters only and matches exactly, later stored counts within 1% (the reference
+    keeps whichever thread wins its atomic race).  The final cost is the reference's."""
     inst = load_fixture(run["file"])
     res = engine.learn(inst, costs=run["costs"], max_cost=run["max_cost"], neg_type=run["neg"],
                        key_mode=api.KEY_REF, rlx_type=run["rlx"], schedule=api.SCHEDULE_PER_BLOCK, limit_traces=True)
     assert res.device_flags & ~1 == 0
     mine = [[b["cost"], b["op"], b["all_before"], b["stored_before"], b["to_check"]] for b in res.blocks]
+    oracle = O.learn(inst, costs=run["costs"], max_cost=run["max_cost"], neg_type=run["neg"], key_mode=run["rlx"],
+                     limit_traces=True)
+    assert mine == [list(p) for p in oracle.progress if p[1] != "A"]
     ref = [p for p in run["progress"] if p[1] != "A"]
     assert len(mine) == len(ref)
     for a, b in zip(mine, ref):
@@ -111,7 +117,19 @@ def test_reference_keys_match_reference_runs(engine, run):
         assert O.formula_cost(res.formula, run["costs"]) == fin["cost"]
     fused = engine.learn(inst, costs=run["costs"], max_cost=run["max_cost"], neg_type=run["neg"],
                          key_mode=api.KEY_REF, rlx_type=run["rlx"], limit_traces=True)
-    assert (fused.status, fused.cost) == (res.status, res.cost)
+    assert (fused.status, fused.cost, fused.all_ltls) == (res.status, res.cost, res.all_ltls)
+    # every level's rows, enumerated to max_cost, are the oracle's representatives
+    full = engine.learn(inst, costs=run["costs"], max_cost=run["max_cost"], neg_type=run["neg"],
+                        key_mode=api.KEY_REF, rlx_type=run["rlx"], limit_traces=True, stop_at_found=False)
+    want = O.learn(inst, costs=run["costs"], max_cost=run["max_cost"], neg_type=run["neg"], key_mode=run["rlx"],
+                   limit_traces=True, stop_at_found=False)
+    starts = engine.level_starts(run["max_cost"] + 2)
+    for c in range(run["costs"][0], run["max_cost"] + 1):
+        theirs = want.level_rows(c)
+        assert starts[c + 1] - starts[c] == len(theirs), c
+        if len(theirs):
+            rows, _ = engine.read_rows(starts[c], len(theirs))
+            assert row_set(rows) == row_set(theirs), c
 
 
 @pytest.mark.parametrize("name", sorted(edge_cases()))

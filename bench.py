@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--cache-gb", type=float, default=6.0, help="language cache per engine")
     ap.add_argument("--slots", type=int, default=20,
                     help="instance slots of the batch call; 0 times the single engine only (profiling runs)")
-    ap.add_argument("--slot-cache-gb", type=float, default=3.0, help="language cache per batch slot")
+    ap.add_argument("--slot-cache-gb", type=float, default=5.0,
+                    help="language cache per batch slot (the largest instance of the batch must fit: 3.9 GB)")
     ap.add_argument("--slot-slots-log2", type=int, default=24, help="hash slots per batch slot")
     ap.add_argument("--slots-log2", type=int, default=27)
     ap.add_argument("--small-rows", type=int, default=1, help="small levels: right rows per warp and item")

@@ -128,6 +128,11 @@ typedef struct ltlg_level_stat {
     uint64_t candidates;       /* candidates the device evaluated at this cost */
     uint64_t uniques;          /* rows stored at this cost */
     double ms;                 /* device time of the level (record_levels) */
+    /* record_levels, fused schedule: microseconds from the end of the level below to this
+       level's plan being published, its first item claimed, its first row begun (0: none) */
+    double plan_us;
+    double claim_us;
+    double start_us;
 } ltlg_level_stat;
 
 typedef struct ltlg_block_stat {

@@ -61,7 +61,7 @@ class Options(C.Structure):
 
 class LevelStat(C.Structure):
     _fields_ = [("cost", C.c_int32), ("blocks", C.c_int32), ("candidates", C.c_uint64), ("uniques", C.c_uint64),
-                ("ms", C.c_double)]
+                ("ms", C.c_double), ("plan_us", C.c_double), ("claim_us", C.c_double), ("start_us", C.c_double)]
 
 
 class BlockStat(C.Structure):
@@ -189,7 +189,8 @@ class LearnResult:
 
 def _result(r: Result) -> LearnResult:
     levels = [dict(cost=r.levels[i].cost, blocks=r.levels[i].blocks, candidates=r.levels[i].candidates,
-                   uniques=r.levels[i].uniques, ms=r.levels[i].ms) for i in range(r.num_levels)]
+                   uniques=r.levels[i].uniques, ms=r.levels[i].ms, plan_us=r.levels[i].plan_us,
+                   claim_us=r.levels[i].claim_us, start_us=r.levels[i].start_us) for i in range(r.num_levels)]
     blocks = [dict(cost=b.cost, op=OPS[b.op], left_cost=b.left_cost, right_cost=b.right_cost,
                    stored_before=b.stored_before, all_before=b.all_before, to_check=b.to_check)
               for b in (r.blocks[i] for i in range(r.num_blocks))]

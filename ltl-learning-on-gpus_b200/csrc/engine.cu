@@ -107,7 +107,7 @@ struct ltlg_engine {
     int n = 0, pitch = 0, nalpha = 0, max_cost = 0;
     long long cap_rows = 0;
     int tile = 0, stages = 0, grid = 0, hk = 0;
-    long long tile_bytes = 0;
+    long long tile_bytes = 0, row_bytes = 0;
     std::vector<long long> level_start;
     std::string last_error;
 };
@@ -198,15 +198,20 @@ void build_string(const std::map<u64, u64> &par, u64 row, u64 p, bool is_root, c
     }
 }
 
-// Level-kernel geometry for rows of `pitch` words: the left tile (shrunk from `want` until at
-// least three item slots fit the shared memory) and the slots.  Returns false when not even one
-// slot of a 2-row tile fits.
-bool geometry(int want, int pitch, int &tile, int &stages, long long &tile_bytes) {
-    constexpr long long BUDGET = 200 * 1024;  // dynamic shared memory for the slots' tiles
+// Level-kernel geometry for rows of `pitch` words.  Rows of at least STAGE_MIN_PITCH words are
+// staged per consumer warp when those buffers and three slots of 2-row tiles fit the shared
+// memory; the rest of the budget holds the slots' tiles: the left tile is shrunk from `want`
+// until at least three slots fit.  Returns false when not even one slot of a 2-row tile fits.
+bool geometry(int want, int pitch, int &tile, int &stages, long long &tile_bytes, long long &row_bytes) {
+    constexpr long long BUDGET = 216 * 1024;  // dynamic shared memory for tiles and staged rows
+    constexpr int STAGE_MIN_PITCH = 128;
+    const long long rb = (long long)pitch * 8;
+    row_bytes = pitch >= STAGE_MIN_PITCH && LEVEL_CONSUMERS * rb + 3 * 2 * rb <= BUDGET ? rb : 0;
+    const long long budget = BUDGET - LEVEL_CONSUMERS * row_bytes;
     tile = want;
-    while (tile > 2 && BUDGET / ((long long)tile * pitch * 8) < 3) tile /= 2;
-    tile_bytes = (long long)tile * pitch * 8;
-    stages = (int)std::min<long long>(8, BUDGET / tile_bytes);
+    while (tile > 2 && budget / ((long long)tile * rb) < 3) tile /= 2;
+    tile_bytes = (long long)tile * rb;
+    stages = (int)std::min<long long>(8, budget / tile_bytes);
     return stages >= 1;
 }
 
@@ -366,6 +371,7 @@ cudaError_t run_levels(ltlg_engine *e, bool persist, int grid, double t0, double
     hl->tile = e->tile;
     hl->stages = e->stages;
     hl->tile_bytes = e->tile_bytes;
+    hl->row_bytes = e->row_bytes;
     cudaStream_t st = e->stream;
     cudaError_t err = cudaMemcpyAsync(e->launch.p, hl, sizeof(Launch), cudaMemcpyHostToDevice, st);
     if (err != cudaSuccess) return err;
@@ -492,21 +498,23 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         res->status = letter_hit >= 0 ? LTLG_FOUND : LTLG_NOT_FOUND;
         res->cost = letter_hit >= 0 ? c1 : std::max(c1, max_cost);
         res->all_ltls = all;
+        res->evaluated = all;
         res->formula = strdup(letter_hit >= 0 ? std::string(1, alpha[letter_hit]).c_str() : "not_found");
         res->seconds = now_s() - t0;
         return res->status;
     }
     if (cap_rows < nalpha + 1) return fail_status(res, LTLG_NO_MEMORY);
     int tile = 0, stages = 0;
-    long long tile_bytes = 0;
-    if (!geometry(e->cfg.left_tile, pitch, tile, stages, tile_bytes)) return fail_status(res, LTLG_BAD_ARGS);
+    long long tile_bytes = 0, row_bytes = 0;
+    if (!geometry(e->cfg.left_tile, pitch, tile, stages, tile_bytes, row_bytes)) return fail_status(res, LTLG_BAD_ARGS);
     const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
-    const size_t smem = level_kernel_smem(stages, tile_bytes);
+    const size_t smem = level_kernel_smem(stages, tile_bytes, row_bytes);
     const int per_sm = level_kernel_ctas_per_sm(hk, smem);
     if (per_sm < 1) return fail_status(res, LTLG_BAD_ARGS);
     e->tile = tile;
     e->stages = stages;
     e->tile_bytes = tile_bytes;
+    e->row_bytes = row_bytes;
     e->hk = hk;
     e->grid = e->num_sms * per_sm;
 
@@ -549,7 +557,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     if ((err = ensure(e->ls, (size_t)ncost * 8)) != cudaSuccess) return fail_cuda(e, err, res);
     if ((err = ensure(e->ne, (size_t)ncost * 4)) != cudaSuccess) return fail_cuda(e, err, res);
     if ((err = ensure(e->lcands, (size_t)ncost * 8)) != cudaSuccess) return fail_cuda(e, err, res);
-    if ((err = ensure(e->lns, (size_t)ncost * 8)) != cudaSuccess) return fail_cuda(e, err, res);
+    if ((err = ensure(e->lns, (size_t)ncost * LEVEL_TRACE * 8)) != cudaSuccess) return fail_cuda(e, err, res);
     if ((err = ensure(e->lstats, (size_t)ncost * LSTATS * 8)) != cudaSuccess) return fail_cuda(e, err, res);
     if ((err = ensure(e->entries, (size_t)(2 * cap_entries) * sizeof(Entry))) != cudaSuccess)
         return fail_cuda(e, err, res);
@@ -559,7 +567,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
             cudaSuccess ||
         (err = ensure_host(e->h_ls, (size_t)ncost * 8)) != cudaSuccess ||
         (err = ensure_host(e->h_lcands, (size_t)ncost * 8)) != cudaSuccess ||
-        (err = ensure_host(e->h_lns, (size_t)ncost * 8)) != cudaSuccess ||
+        (err = ensure_host(e->h_lns, (size_t)ncost * LEVEL_TRACE * 8)) != cudaSuccess ||
         (err = ensure_host(e->h_snaps, (size_t)cap_entries * 8)) != cudaSuccess ||
         (err = ensure_host(e->h_win, (size_t)(2 * cap_entries + 2) * 8)) != cudaSuccess ||
         (err = ensure_host(e->h_entries, (size_t)cap_entries * sizeof(Entry))) != cudaSuccess)
@@ -582,7 +590,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     }
     cudaMemsetAsync(e->ls.p, 0, (size_t)ncost * 8, st);
     cudaMemsetAsync(e->lcands.p, 0, (size_t)ncost * 8, st);
-    cudaMemsetAsync(e->lns.p, 0, (size_t)ncost * 8, st);
+    cudaMemsetAsync(e->lns.p, 0, (size_t)ncost * LEVEL_TRACE * 8, st);
     if (want_stats) cudaMemsetAsync(e->lstats.p, 0, (size_t)ncost * LSTATS * 8, st);
     InstCtl *hc = (InstCtl *)e->h_ctl.p;
     memset(hc, 0, sizeof(InstCtl));
@@ -772,7 +780,7 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     // ---- level ranges, statistics, the reference's candidate count
     cudaMemcpyAsync(e->h_ls.p, e->ls.p, (size_t)ncost * 8, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(e->h_lcands.p, e->lcands.p, (size_t)ncost * 8, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(e->h_lns.p, e->lns.p, (size_t)ncost * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(e->h_lns.p, e->lns.p, (size_t)ncost * LEVEL_TRACE * 8, cudaMemcpyDeviceToHost, st);
     if ((err = read_ctl(e, hc)) != cudaSuccess) return fail_cuda(e, err, res);
     const long long rows_final = std::min<long long>((long long)hc->row_count, cap_rows);
     const long long *hls = (const long long *)e->h_ls.p;
@@ -795,8 +803,16 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
         L.cost = c;
         L.candidates = hlc[c];
         L.uniques = (uint64_t)(ls[c + 1] - ls[c]);
-        if (hns[c] && prev_ns) L.ms = (double)(hns[c] - prev_ns) * 1e-6;
-        if (hns[c]) prev_ns = hns[c];
+        const u64 *tr = hns + (size_t)c * LEVEL_TRACE;
+        const u64 end = tr[LT_END];
+        if (end && prev_ns) {
+            L.ms = (double)(end - prev_ns) * 1e-6;
+            auto since = [&](u64 t) { return t >= prev_ns ? (double)(t - prev_ns) * 1e-3 : 0.0; };
+            if (tr[LT_PUBLISHED]) L.plan_us = since(tr[LT_PUBLISHED]);
+            if (tr[LT_CLAIMED]) L.claim_us = since(tr[LT_CLAIMED]);
+            if (tr[LT_STARTED]) L.start_us = since(tr[LT_STARTED]);
+        }
+        if (end) prev_ns = end;
         lstats.push_back(L);
     }
     // all_ltls: whole levels before the level of the find, then that level's blocks in the
@@ -955,6 +971,7 @@ LTLG_API int ltlg_engine_label_blocks(ltlg_engine *e, const ltlg_traces *t, cons
     A.plan_flags = PLAN_UNFUSED;
     A.stop_at_found = 0;
     A.find_first = 0;
+    A.max_cost = c;  // the window that finishes level c plans nothing after it
     cudaMemcpyAsync(e->ctl.p, hc, sizeof(InstCtl), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(e->args.p, &A, sizeof(InstArgs), cudaMemcpyHostToDevice, st);
     err = launch_plan_level(dA, c, st);
@@ -1198,9 +1215,10 @@ LTLG_API int ltlg_batch_learn(ltlg_batch *b, const ltlg_traces *traces, int32_t 
         const bool keyed = opt->key_mode != LTLG_KEY_EXACT;
         const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
         int tile = 0, stages = 0;
-        long long tile_bytes = 0;
-        if (!geometry(b->cfg.left_tile, max_pitch, tile, stages, tile_bytes)) err = cudaErrorInvalidValue;
-        const int per_sm = err == cudaSuccess ? level_kernel_ctas_per_sm(hk, level_kernel_smem(stages, tile_bytes)) : 0;
+        long long tile_bytes = 0, row_bytes = 0;
+        if (!geometry(b->cfg.left_tile, max_pitch, tile, stages, tile_bytes, row_bytes)) err = cudaErrorInvalidValue;
+        const int per_sm =
+            err == cudaSuccess ? level_kernel_ctas_per_sm(hk, level_kernel_smem(stages, tile_bytes, row_bytes)) : 0;
         if (per_sm < 1 && err == cudaSuccess) err = cudaErrorInvalidConfiguration;
         const int grid = b->num_sms * std::max(per_sm, 1);
         // inputs: instance records, steps and offsets of every instance in one array each
@@ -1325,6 +1343,7 @@ LTLG_API int ltlg_batch_learn(ltlg_batch *b, const ltlg_traces *traces, int32_t 
             L.tile = tile;
             L.stages = stages;
             L.tile_bytes = tile_bytes;
+            L.row_bytes = row_bytes;
             cudaStream_t st = b->stream;
             err = cudaMemcpyAsync(b->bin.p, b->h_bin.p, (size_t)nd * sizeof(BatchIn), cudaMemcpyHostToDevice, st);
             if (err == cudaSuccess && total_steps)

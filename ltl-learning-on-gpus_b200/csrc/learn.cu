@@ -46,6 +46,7 @@ constexpr int OP_ANDOR_CLASS = 8;              // binary_row's class of & and | 
 constexpr int ENTRY_CACHE = 256;               // item starts of a plan's first entries kept in shared memory
 constexpr int NWARPS = LEVEL_THREADS / 32;
 constexpr int NCONS = NWARPS - 1;              // consumer warps per CTA
+static_assert(NCONS == LEVEL_CONSUMERS, "consumer warps");
 constexpr u64 PIPE_WAIT_NS = 30000000000ull;   // a consumer's wait for the producer (beyond every producer bound)
 constexpr u64 EMPTY_WAIT_NS = 10000000000ull;  // the producer's wait for the consumers to leave a slot
 constexpr u64 STALL_NS = 4000000000ull;        // no level progress while waiting for the next plan
@@ -71,7 +72,7 @@ struct Slot {
     int check_only;
     int stop;                 // remaining rows are skipped (a find at or before this entry)
     int inst;                 // the item's instance (index into Launch::args)
-    int pad;
+    int trace_first;          // the producer's first item of this plan (level stamps)
     InstArgs args;            // its arguments as they were when the item was claimed (a batch slot's
                               // arguments change when it takes the next instance)
 };
@@ -79,13 +80,14 @@ struct Slot {
 // ---------------------------------------------------------------- candidate generators
 // pre(c) loads what every candidate of the set shares at chunk c (binary: the right row;
 // unary: the word metadata); word(t, c, pre) gives words 2c, 2c+1 of candidate t.
-template <int OPC>
+// ST: the right (or source) row is staged in shared memory, else it is read from the cache.
+template <int OPC, bool ST>
 struct BinGen {
     const ulonglong2 *left;   // shared-memory tile, row stride nch
-    const ulonglong2 *right;  // global right row
+    const ulonglong2 *right;  // right row (shared memory when ST)
     int nch;
     int rop;
-    __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldcg(right + c); }
+    __device__ __forceinline__ ulonglong2 pre(int c) const { return ST ? right[c] : __ldcg(right + c); }
     __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 r) const {
         if (OPC == OP_U) {
             const ulonglong2 l = left[(t >> 1) * nch + c];
@@ -99,12 +101,13 @@ struct BinGen {
 };
 
 // Candidate t of a fused unary row: operator slot t (0 ~, 1 X, 2 F, 3 G) of one source row.
+template <bool ST>
 struct UnGen {
-    const ulonglong2 *src;
+    const ulonglong2 *src;   // source row (shared memory when ST)
     const ulonglong2 *meta;
-    __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldg(meta + c); }
+    __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldcg(meta + c); }
     __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 m) const {
-        const ulonglong2 s = __ldcg(src + c);
+        const ulonglong2 s = ST ? src[c] : __ldcg(src + c);
         const int op = unary_slot_op(t);
         return make_ulonglong2(unary_word(op, s.x, m.x & LENMASK), unary_word(op, s.y, m.y & LENMASK));
     }
@@ -193,13 +196,15 @@ __device__ __forceinline__ void count_row_stats(u64 *cnt, bool stored, u32 pmiss
 // candidates concerned, so their loads are in flight together.  Claims are written and
 // published before any lane waits on another warp's publication, so waits cannot cycle.
 // The reference's relaxed keys keep, of the CSs that share a key in a level, the one its
-// threads insert first: blocks run in order and, within a block, thread order (the oracle's
-// tid order, which the reference's recorded runs follow).  Here the row of a key records the
-// priority (block position << 40 | the reference's thread index, U's "l U r" before "r U l")
-// of the candidate it holds; a candidate of the same level with the same key and a lower
-// priority takes the row over: it locks the priority word (bit 0), rewrites the row and its
-// parent, and publishes its priority.  Rows of lower levels are never taken over.  One lane,
-// bounded waits.
+// threads insert first: blocks run in order and, within a block, roughly thread order (the
+// oracle's sequential tid order).  Here the row of a key records the priority (block position
+// << 40 | the reference's thread index, U's "l U r" before "r U l") of the candidate it holds;
+// a candidate of the same level with the same key and a lower priority takes the row over: it
+// locks the priority word (bit 0), rewrites the row and its parent, and publishes its
+// priority.  Rows of lower levels are never taken over.  So a shared key never goes to a later
+// block, which keeps the per-block stored counts equal to the oracle's; inside a block the
+// thread index counts operand rows in the order they were stored, which on the device (as in
+// the reference) is the order warps reached the hash set.  One lane, bounded waits.
 template <class Gen>
 __device__ void take_over(const InstArgs &A, InstCtl *C, const Gen &g, int t, u64 row, u64 prio, u64 parent) {
     u64 *pw = A.prio + row;
@@ -387,6 +392,10 @@ __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost,
 template <int NC, class Gen, class ParentOf, class PosOf, class TidOf>
 __device__ __forceinline__ void finish(const InstArgs &A, InstCtl *C, Slot &sl, const Gen &g, u64 (&h)[NC], u32 bp,
                                        u32 bn, u32 valid, ParentOf parent_of, PosOf pos_of, TidOf tid_of, int lane) {
+    // once the language cache has overflowed, the level's remaining CSs are not stored and take
+    // no hash slots (loaded first: its latency hides behind the reduction)
+    u32 st = 0;
+    if (lane == 0 && !sl.check_only) st = *(volatile const u32 *)&C->status;
     const u64 sum = reduce_to_lane<NC>(h, lane);
     const u32 anyp = __reduce_or_sync(FULL, bp), anyn = __reduce_or_sync(FULL, bn);
     const u32 acc = ~(anyp | anyn) & valid;
@@ -400,7 +409,8 @@ __device__ __forceinline__ void finish(const InstArgs &A, InstCtl *C, Slot &sl, 
                 atomicCAS(A.found_par + p, 0ull, (1ull << 63) | myparent);
                 atomicMin(&C->found_key, key);
             }
-            if (A.find_first || sl.pos >= p) sl.stop = 1;
+            // the item's remaining rows are skipped only when the search ends at this level
+            if (A.stop_at_found && (A.find_first || sl.pos >= p)) sl.stop = 1;
         }
         __syncwarp();
         if (A.stop_at_found) return;  // this level is the last one; its candidates need no dedupe
@@ -422,21 +432,22 @@ __device__ __forceinline__ void finish(const InstArgs &A, InstCtl *C, Slot &sl, 
         fp = fmix64(kh ^ fmix64(kl + 0x5ad0dedull));
     }
     const u64 prio = A.prio && ((valid >> lane) & 1u) ? ((u64)(u32)pos_of(lane) << 40) | tid_of(lane) : 0ull;
-    resolve<NC>(A, C, cost, g, fp, (valid >> lane) & 1u, myparent, kh, kl, prio, anyp, anyn, lane);
+    const bool room = (__shfl_sync(FULL, st, 0) & ST_OVERFLOW) == 0u;
+    resolve<NC>(A, C, cost, g, fp, room && ((valid >> lane) & 1u), myparent, kh, kl, prio, anyp, anyn, lane);
 }
 
 // ---------------------------------------------------------------- rows
-// Binary row: right row r against the slot's tile of TLP left rows (U: both orders of each
-// pair, TL = 2 TLP candidates; & and |: TL = TLP).  Chunks are 16 bytes (two words); four are
-// in flight per lane.  Positives are the first npos words, so acceptance needs no metadata.
-template <int OPC, int TL, int HK>
-__device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &sl, const ulonglong2 *tile, long long r,
-                                           int lane) {
+// Binary row: right row r (at R: in the cache, or the warp's staged copy with ST) against the
+// slot's tile of TLP left rows (U: both orders of each pair, TL = 2 TLP candidates; & and |:
+// TL = TLP).  Chunks are 16 bytes (two words); four are in flight per lane.  Positives are the
+// first npos words, so acceptance needs no metadata.
+template <int OPC, int TL, int HK, bool ST>
+__device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &sl, const ulonglong2 *tile,
+                                           const ulonglong2 *R, long long r, int lane) {
     constexpr int TLP = OPC == OP_U ? TL / 2 : TL;
     constexpr int NC = TL;
     const int nch = A.pitch >> 1, npos = A.npos, n = A.n;
     const int nl = sl.nl, rop = sl.op;
-    const ulonglong2 *R = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)r * A.pitch);
     u64 h[NC];
 #pragma unroll
     for (int t = 0; t < NC; ++t) h[t] = 0;
@@ -446,7 +457,7 @@ __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int c = c0 + 32 * u;
-            if (c < nch) rvv[u] = __ldcg(R + c);
+            if (c < nch) rvv[u] = ST ? R[c] : __ldcg(R + c);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -483,7 +494,7 @@ __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &
     }
     const int cnt = OPC == OP_U ? 2 * nl : nl;
     const u32 valid = cnt >= 32 ? FULL : ((1u << cnt) - 1u);
-    const BinGen<OPC> g{tile, R, nch, rop};
+    const BinGen<OPC, ST> g{tile, R, nch, rop};
     const long long l_first = sl.l_first;
     finish<NC>(A, C, sl, g, h, bp, bn, valid,
                [&](int t) {
@@ -503,14 +514,15 @@ __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &
     if (lane == 0) atomicAdd(&sl.evals, (unsigned)cnt);
 }
 
-// Unary row: every operator of the slot's mask on source row s (one load of each chunk).
-template <int HK>
-__device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &sl, long long s, int lane) {
+// Unary row: every operator of the slot's mask on source row s (at src: in the cache, or the
+// warp's staged copy with ST; one load of each chunk).
+template <int HK, bool ST>
+__device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &sl, const ulonglong2 *src, long long s,
+                                          int lane) {
     constexpr int NC = 4;
     const int nch = A.pitch >> 1, npos = A.npos, n = A.n;
     const int mask = sl.op;
     const ulonglong2 *meta = reinterpret_cast<const ulonglong2 *>(A.wmeta);
-    const ulonglong2 *src = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)s * A.pitch);
     u64 h[NC] = {0, 0, 0, 0};
     u32 bp = 0, bn = 0;
     for (int c0 = lane; c0 < nch; c0 += 64) {
@@ -519,8 +531,8 @@ __device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &s
         for (int u = 0; u < 2; ++u) {
             const int c = c0 + 32 * u;
             if (c < nch) {
-                sv[u] = __ldcg(src + c);
-                mv[u] = __ldg(meta + c);
+                sv[u] = ST ? src[c] : __ldcg(src + c);
+                mv[u] = __ldcg(meta + c);  // a batch slot rewrites its metadata in the launch
             }
         }
 #pragma unroll
@@ -544,7 +556,7 @@ __device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &s
         }
     }
     const u32 valid = (u32)(mask & 15);
-    const UnGen g{src, meta};
+    const UnGen<ST> g{src, meta};
     finish<NC>(A, C, sl, g, h, bp, bn, valid,
                [&](int t) { return pack_parent(unary_slot_op(t & 3), (u64)s, 0); },
                [&](int t) { return sl.upos[t & 3]; }, [&](int) -> u64 { return (u64)(s - sl.e_r0); }, lane);
@@ -861,7 +873,7 @@ __device__ __forceinline__ void publish(InstCtl *C, long long items, bool open) 
 // stopping when the search is over.  Levels without any block are closed on the spot.  One
 // warp (all lanes).  With open false (host-driven levels) the next plan is made but hands out
 // nothing until the host opens it.
-__device__ bool close_level(const InstArgs &A, InstCtl *C, bool open, int lane) {
+__device__ __noinline__ bool close_level(const InstArgs &A, InstCtl *C, bool open, int lane) {
     __threadfence();
     int c = (int)__ldcg(&C->plan.cost);
     bool halt = false;
@@ -874,7 +886,7 @@ __device__ bool close_level(const InstArgs &A, InstCtl *C, bool open, int lane) 
                 A.ne[k] = c;
                 C->ne_count = k + 1;
             }
-            if (A.level_ns) A.level_ns[c] = globaltimer();
+            if (A.level_ns) A.level_ns[(u64)c * LEVEL_TRACE + LT_END] = globaltimer();
             C->last_cost = (u32)c;
             const u64 fk = __ldcg(&C->found_key);
             if (fk != NO_FIND && (int)(fk >> 32) == c && __ldcg(&C->found) == 0ull) {
@@ -903,7 +915,10 @@ __device__ bool close_level(const InstArgs &A, InstCtl *C, bool open, int lane) 
         if (A.plan_flags & PLAN_LEARNED) score_plan(A, C, lane);
         const long long items = __ldcg(&C->plan.items);
         if (items > 0) {
-            if (lane == 0) publish(C, items, open);
+            if (lane == 0) {
+                publish(C, items, open);
+                if (A.level_ns) A.level_ns[(u64)c * LEVEL_TRACE + LT_PUBLISHED] = globaltimer();
+            }
             __syncwarp();
             return false;
         }
@@ -1075,7 +1090,7 @@ __device__ bool setup_instance(BatchDev &B, int s, int idx, int lane) {
             o.cost = hit >= 0 ? c1 : max(c1, A.max_cost);
             o.all_ltls = all;
             o.evaluated = all;
-            o.rows = hit >= 0 ? hit + 1 : 0;
+            o.rows = hit >= 0 && A.stop_at_found ? hit + 1 : 0;  // no rows of an instance without traces
             o.device_flags = 0;
             o.ns = globaltimer() - B.t0[s];
             __threadfence();
@@ -1274,6 +1289,7 @@ struct ProdCache {
     int cur;              // entry in `e`
     int rc, ur, cost, check_only;
     long long plan_items;
+    int trace_first;      // the next item filled is this producer's first of the plan
     long long item0[ENTRY_CACHE];
     Entry e;
     InstArgs a;           // the instance's arguments (read once per plan)
@@ -1297,7 +1313,7 @@ __device__ __forceinline__ bool launch_done(const Launch &L, int lane) {
 
 // The producer warp: claims items, fills slots, issues the tile copies and the L2 prefetches.
 template <int TL>
-__device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int lane) {
+__device__ __noinline__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int lane) {
     __shared__ ProdCache pc;
     const int S = L.stages;
     const long long tile_words = L.tile_bytes / 8;
@@ -1426,6 +1442,8 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
                 pc.cost = cost;
                 pc.check_only = chk;
                 pc.plan_items = pitems;
+                pc.trace_first = pc.a.level_ns != nullptr;
+                if (pc.trace_first) atomicCAS(pc.a.level_ns + (u64)cost * LEVEL_TRACE + LT_CLAIMED, 0ull, globaltimer());
             }
             __syncwarp();
         }
@@ -1459,6 +1477,8 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
         if (lane == 0) {
             const u32 bytes = fill_slot(sl, inst, pc.e, item, L.tile, pc.rc, pc.ur, pc.cost, pc.check_only,
                                         pc.plan_items, skip, pc.a.pitch);
+            sl.trace_first = pc.trace_first;
+            pc.trace_first = 0;
             if (!skip) {
                 const u64 pitch = (u64)pc.a.pitch;
                 const u64 rows_bytes = (u64)sl.nrows * pitch * 8;
@@ -1487,11 +1507,86 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
     __syncwarp();
 }
 
-// A consumer warp: takes the rows of the slots in order until the producer's end slot.
-template <int TL, int HK>
-__device__ void consumer(const Launch &L, unsigned char *smem, const u64 *tiles, int lane) {
+// The rows of one slot a consumer warp takes, until the slot has none left.  With ST every row
+// is first copied into the warp's own shared-memory buffer `wrow` (one bulk copy, mbarrier
+// `wbar`, phase *wph), so the candidate words of the row, of the claims and of the
+// verifications come from shared memory.  Returns SLOT_CLOSE when this warp finished the
+// level's last item, SLOT_FAIL after a copy that did not arrive, else SLOT_NEXT.  No calls: the
+// cold work (closing a level, a batch slot's next instance) is the caller's, so the row loop
+// keeps its registers.
+enum { SLOT_NEXT = 0, SLOT_CLOSE = 1, SLOT_FAIL = 2 };
+template <int TL, int HK, bool ST>
+__device__ __noinline__ int take_rows(Slot &sl, int kind, const ulonglong2 *tile, u64 *wrow, u64 *wbar, u32 *wph,
+                                      int lane) {
+    const InstArgs &A = sl.args;
+    InstCtl *C = A.ctl;
+    bool fenced = false;
+    int out = SLOT_NEXT;
+    for (;;) {
+        unsigned idx = 0;
+        if (lane == 0) idx = atomicAdd(&sl.next_row, 1u);
+        idx = __shfl_sync(FULL, idx, 0);
+        if ((int)idx >= sl.nrows) break;
+        if (idx == 0 && sl.trace_first && lane == 0)
+            atomicCAS(A.level_ns + (u64)sl.cost * LEVEL_TRACE + LT_STARTED, 0ull, globaltimer());
+        if (!*(volatile int *)&sl.stop) {
+            const long long r = sl.row0 + idx;
+            const ulonglong2 *rp = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)r * A.pitch);
+            if (ST) {
+                bool ok = true;
+                if (lane == 0) {
+                    // rows of the finished levels were written through the generic proxy
+                    if (!fenced) fence_proxy_async_global();
+                    fence_proxy_async();  // the warp's reads of the previous staged row come first
+                    const u32 bytes = (u32)A.pitch * 8u;
+                    mbar_expect_tx(wbar, bytes);
+                    bulk_g2s(wrow, rp, bytes, wbar);
+                    ok = mbar_wait_for(wbar, *wph, PIPE_WAIT_NS);
+                    if (!ok) {
+                        atomicOr(&C->status, ST_TMA);
+                        mbar_wait_for(wbar, *wph, PIPE_WAIT_NS);  // the copy in flight, before leaving
+                    }
+                }
+                fenced = true;
+                *wph ^= 1u;
+                if (!__shfl_sync(FULL, ok, 0)) return SLOT_FAIL;
+                rp = reinterpret_cast<const ulonglong2 *>(wrow);
+            }
+            if (kind == ENT_UNARY)
+                unary_row<HK, ST>(A, C, sl, rp, r, lane);
+            else if (kind == ENT_ANDOR)
+                binary_row<OP_ANDOR_CLASS, TL, HK, ST>(A, C, sl, tile, rp, r, lane);
+            else
+                binary_row<OP_U, TL, HK, ST>(A, C, sl, tile, rp, r, lane);
+            if (ST) __syncwarp();  // every lane is done with the staged row before the next copy
+        }
+        unsigned d = 0;
+        __threadfence_block();  // this row's evals count is in before the row counts as done
+        if (lane == 0) d = atomicAdd(&sl.rows_done, 1u);
+        d = __shfl_sync(FULL, d, 0);
+        if ((int)d + 1 == sl.nrows) {  // the item is done
+            u64 dd = 0;
+            if (lane == 0) {
+                const unsigned ev = atomicAdd(&sl.evals, 0u);
+                if (ev) atomicAdd(&C->evaluated, (u64)ev);
+                __threadfence();
+                dd = atomicAdd(&C->done, 1ull);
+            }
+            dd = __shfl_sync(FULL, dd, 0);
+            if ((long long)dd + 1 == sl.plan_items) out = SLOT_CLOSE;
+        }
+    }
+    return out;
+}
+
+// A consumer warp: takes the rows of the slots in order until the producer's end slot; the
+// warp that finishes a level's last item closes the level (and plans the next one).
+template <int TL, int HK, bool ST>
+__device__ __noinline__ void consumer(const Launch &L, unsigned char *smem, const u64 *tiles, u64 *wrow, u64 *wbar,
+                                      int lane) {
     const int S = L.stages;
     const long long tile_words = L.tile_bytes / 8;
+    u32 wph = 0;  // phase of wbar
     for (u64 k = 0;; ++k) {
         const int s = (int)(k % (u64)S);
         Slot &sl = *slot_at(smem, s);
@@ -1504,46 +1599,16 @@ __device__ void consumer(const Launch &L, unsigned char *smem, const u64 *tiles,
         }
         const int kind = *(volatile int *)&sl.kind;
         if (kind == 0) return;
-        const InstArgs &A = sl.args;
-        InstCtl *C = A.ctl;
         const ulonglong2 *tile = reinterpret_cast<const ulonglong2 *>(tiles + (u64)s * tile_words);
+        const int got = take_rows<TL, HK, ST>(sl, kind, tile, wrow, wbar, &wph, lane);
+        if (got == SLOT_FAIL) return;
         int recycle = -1;  // a batch slot whose instance's search ended in this warp
-        for (;;) {
-            unsigned idx = 0;
-            if (lane == 0) idx = atomicAdd(&sl.next_row, 1u);
-            idx = __shfl_sync(FULL, idx, 0);
-            if ((int)idx >= sl.nrows) break;
-            if (!*(volatile int *)&sl.stop) {
-                const long long r = sl.row0 + idx;
-                if (kind == ENT_UNARY)
-                    unary_row<HK>(A, C, sl, r, lane);
-                else if (kind == ENT_ANDOR)
-                    binary_row<OP_ANDOR_CLASS, TL, HK>(A, C, sl, tile, r, lane);
-                else
-                    binary_row<OP_U, TL, HK>(A, C, sl, tile, r, lane);
-            }
-            unsigned d = 0;
-            __threadfence_block();  // this row's evals count is in before the row counts as done
-            if (lane == 0) d = atomicAdd(&sl.rows_done, 1u);
-            d = __shfl_sync(FULL, d, 0);
-            if ((int)d + 1 == sl.nrows) {  // the item is done
-                u64 dd = 0;
-                if (lane == 0) {
-                    const unsigned ev = atomicAdd(&sl.evals, 0u);
-                    if (ev) atomicAdd(&C->evaluated, (u64)ev);
-                    __threadfence();
-                    dd = atomicAdd(&C->done, 1ull);
-                }
-                dd = __shfl_sync(FULL, dd, 0);
-                if ((long long)dd + 1 == sl.plan_items) {
-                    const bool ended = close_level(A, C, L.persist != 0, lane);
-                    if (ended && L.batch) recycle = sl.inst;
-                }
-            }
+        if (got == SLOT_CLOSE) {  // the slot's arguments are read before the slot is released
+            const bool ended = close_level(sl.args, sl.args.ctl, L.persist != 0, lane);
+            if (ended && L.batch) recycle = sl.inst;
         }
         if (lane == 0) mbar_arrive(&sl.empty);
         __syncwarp();
-        // the slot's next instance, outside the row loop (it takes a while and few values are live here)
         if (recycle >= 0) next_instance<HK>(*L.batch, recycle, true, lane);
     }
 }
@@ -1555,10 +1620,11 @@ namespace {
 
 __device__ __forceinline__ size_t slots_bytes(int S) { return ((size_t)S * sizeof(Slot) + 127) & ~(size_t)127; }
 
-template <int TL, int HK>
+template <int TL, int HK, bool ST>
 __global__ void __launch_bounds__(LEVEL_THREADS, 1) level_kernel(const Launch *__restrict__ Lp) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ Launch L;
+    __shared__ __align__(8) u64 wbar[NCONS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         L = *Lp;
@@ -1567,14 +1633,18 @@ __global__ void __launch_bounds__(LEVEL_THREADS, 1) level_kernel(const Launch *_
             mbar_init(&sl.full, 1);
             mbar_init(&sl.empty, NCONS);
         }
+        if (ST)
+            for (int w = 0; w < NCONS; ++w) mbar_init(&wbar[w], 1);
         fence_mbar_init();
     }
     __syncthreads();
     u64 *tiles = reinterpret_cast<u64 *>(smem + slots_bytes(L.stages));
-    if (warp == 0)
+    if (warp == 0) {
         producer<TL>(L, smem, tiles, lane);
-    else
-        consumer<TL, HK>(L, smem, tiles, lane);
+    } else {
+        u64 *rows = tiles + (u64)L.stages * (u64)(L.tile_bytes / 8);
+        consumer<TL, HK, ST>(L, smem, tiles, rows + (u64)(warp - 1) * (u64)(L.row_bytes / 8), &wbar[warp - 1], lane);
+    }
 }
 
 // A batch's first instances: block s sets slot s up (one warp per slot).
@@ -1804,7 +1874,7 @@ __global__ void eval_formula_kernel(const int *__restrict__ prog, int len, const
 
 // The dynamic shared-memory limit is a per-device function attribute: each device keeps the
 // largest size enabled on it so far.
-template <int TL, int HK>
+template <int TL, int HK, bool ST>
 cudaError_t smem_attr(size_t smem) {
     constexpr int MAX_DEVICES = 64;
     static std::atomic<long long> attr_set[MAX_DEVICES];
@@ -1813,7 +1883,7 @@ cudaError_t smem_attr(size_t smem) {
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev >= 0 && dev < MAX_DEVICES && (long long)smem <= attr_set[dev].load()) return cudaSuccess;
-    e = cudaFuncSetAttribute(level_kernel<TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(level_kernel<TL, HK, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess && dev >= 0 && dev < MAX_DEVICES) {
         long long cur = attr_set[dev].load();
         while (cur < (long long)smem && !attr_set[dev].compare_exchange_weak(cur, (long long)smem)) {
@@ -1822,43 +1892,48 @@ cudaError_t smem_attr(size_t smem) {
     return e;
 }
 
-template <int TL, int HK>
+template <int TL, int HK, bool ST>
 cudaError_t launch_tl(const Launch &h, const Launch *d, int grid, cudaStream_t s) {
-    const size_t smem = level_kernel_smem(h.stages, h.tile_bytes);
-    cudaError_t e = smem_attr<TL, HK>(smem);
+    const size_t smem = level_kernel_smem(h.stages, h.tile_bytes, h.row_bytes);
+    cudaError_t e = smem_attr<TL, HK, ST>(smem);
     if (e != cudaSuccess) return e;
-    level_kernel<TL, HK><<<grid, LEVEL_THREADS, smem, s>>>(d);
+    level_kernel<TL, HK, ST><<<grid, LEVEL_THREADS, smem, s>>>(d);
     return cudaGetLastError();
 }
 
-template <int TL, int HK>
+template <int TL, int HK, bool ST>
 int occupancy_tl(size_t smem) {
-    if (smem_attr<TL, HK>(smem) != cudaSuccess) return 0;
+    if (smem_attr<TL, HK, ST>(smem) != cudaSuccess) return 0;
     int n = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<TL, HK>, LEVEL_THREADS, smem) == cudaSuccess
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<TL, HK, ST>, LEVEL_THREADS, smem) ==
+                   cudaSuccess
                ? n
                : 0;
 }
 
+template <int HK, bool ST>
+cudaError_t launch_hk(const Launch &h, const Launch *d, int grid, cudaStream_t s) {
+    return h.tile == 2   ? launch_tl<2, HK, ST>(h, d, grid, s)
+           : h.tile == 4 ? launch_tl<4, HK, ST>(h, d, grid, s)
+                         : launch_tl<8, HK, ST>(h, d, grid, s);
+}
+
 }  // namespace
 
-size_t level_kernel_smem(int stages, long long tile_bytes) {
-    return (((size_t)stages * sizeof(Slot) + 127) & ~(size_t)127) + (size_t)stages * (size_t)tile_bytes;
+size_t level_kernel_smem(int stages, long long tile_bytes, long long row_bytes) {
+    return (((size_t)stages * sizeof(Slot) + 127) & ~(size_t)127) + (size_t)stages * (size_t)tile_bytes +
+           (size_t)NCONS * (size_t)row_bytes;
 }
 
 cudaError_t launch_levels(const Launch &h, const Launch *d, int grid, int hk, cudaStream_t s) {
-    if (hk == 1)
-        return h.tile == 2 ? launch_tl<2, 1>(h, d, grid, s)
-               : h.tile == 4 ? launch_tl<4, 1>(h, d, grid, s)
-                             : launch_tl<8, 1>(h, d, grid, s);
-    return h.tile == 2 ? launch_tl<2, 0>(h, d, grid, s)
-           : h.tile == 4 ? launch_tl<4, 0>(h, d, grid, s)
-                         : launch_tl<8, 0>(h, d, grid, s);
+    const bool st = h.row_bytes > 0;
+    if (hk == 1) return st ? launch_hk<1, true>(h, d, grid, s) : launch_hk<1, false>(h, d, grid, s);
+    return st ? launch_hk<0, true>(h, d, grid, s) : launch_hk<0, false>(h, d, grid, s);
 }
 
 int level_kernel_ctas_per_sm(int hk, size_t smem) {
     // every tile instance has the same resource use up to its registers; ask the 8-row one
-    return hk == 1 ? occupancy_tl<8, 1>(smem) : occupancy_tl<8, 0>(smem);
+    return hk == 1 ? occupancy_tl<8, 1, true>(smem) : occupancy_tl<8, 0, true>(smem);
 }
 
 cudaError_t launch_first_plan(const InstArgs *d, int ninst, int open, cudaStream_t s) {

@@ -117,6 +117,10 @@ enum : int {
 };
 
 // The constant arguments of one instance's learn (device memory).
+// Per-level pipeline stamps (InstArgs::level_ns), LEVEL_TRACE words per cost.
+constexpr int LEVEL_TRACE = 4;
+enum { LT_END = 0, LT_PUBLISHED = 1, LT_CLAIMED = 2, LT_STARTED = 3 };
+
 struct InstArgs {
     int n;               // traces = words per CS
     int pitch;           // words per cache row (n rounded up to a multiple of 4)
@@ -153,7 +157,8 @@ struct InstArgs {
     long long *ls;       // level starts, max_cost + 2 entries: rows of cost c are [ls[c], ls[c + 1])
     int *ne;             // costs of the non-empty levels, increasing (InstCtl::ne_count of them)
     u64 *level_cands;    // per cost
-    u64 *level_ns;       // per cost: globaltimer when the level ended (or null)
+    u64 *level_ns;       // per cost, LEVEL_TRACE globaltimer stamps (or null): the level ended,
+                         // its plan was published, its first item was claimed, its first row began
     u64 *lstats;         // per cost, LSTATS counts of stored rows by their position-0 behaviour (or null)
     Entry *entries;      // the current plan's entries
     u64 *found_par;      // per block position of the current level: (1 << 63) | parents of an accepting candidate
@@ -218,6 +223,8 @@ struct Launch {
     int tile;                // left rows staged per binary item (U: tile / 2 left rows, two candidates each)
     int stages;              // item slots in flight per CTA
     long long tile_bytes;    // shared-memory bytes of one slot's tile
+    long long row_bytes;     // > 0: every consumer warp copies the right (unary: source) row of each
+                             // candidate set into its own shared-memory buffer of this size first
 };
 
 // The feature inputs of a block (operator op) of level c: the same code on the device
@@ -251,10 +258,12 @@ __host__ __device__ inline BlockInfo block_info(int op, int c, int lcost, long l
     return bi;
 }
 
-// Shared memory of one CTA of the level kernel for `stages` slots of tile_bytes each.
-size_t level_kernel_smem(int stages, long long tile_bytes);
 // Threads per CTA of the level kernel (one producer warp and the consumer warps).
 constexpr int LEVEL_THREADS = 512;
+constexpr int LEVEL_CONSUMERS = LEVEL_THREADS / 32 - 1;
+// Shared memory of one CTA of the level kernel: `stages` slots of tile_bytes each, and (row_bytes
+// > 0) one staged row per consumer warp.
+size_t level_kernel_smem(int stages, long long tile_bytes, long long row_bytes);
 
 // Launch wrappers (learn.cu).  The kernels read their arguments from device memory, so a
 // launch (or a captured graph) stays valid while the arguments change between learns.

@@ -235,7 +235,7 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
     int num_sms = 0;
     cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
-    const int per_sm = level_kernel_ctas_per_sm(hk, level_kernel_smem(stages, tile_bytes));
+    const int per_sm = level_kernel_ctas_per_sm(hk, level_kernel_smem(stages, tile_bytes, 0));
     const int grid = (num_sms > 0 ? num_sms : 1) * (per_sm > 0 ? per_sm : 1);
 
     // Inputs and zeroed state (default stream, synchronous copies from stack arrays).
@@ -301,6 +301,7 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     L.tile = tile;
     L.stages = stages;
     L.tile_bytes = tile_bytes;
+    L.row_bytes = 0;  // rows of at most 64 words: read in place
     if ((err = cudaMemcpy(dargs, &A, sizeof(A), cudaMemcpyHostToDevice)) != cudaSuccess ||
         (err = cudaMemcpy(dlaunch, &L, sizeof(L), cudaMemcpyHostToDevice)) != cudaSuccess)
         return LTLG_CUDA_ERROR;
@@ -310,8 +311,9 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     if ((err = launch_levels(L, dlaunch, grid, hk, 0)) != cudaSuccess) return LTLG_CUDA_ERROR;
     if ((err = cudaMemcpy(&hc, ctl, sizeof(hc), cudaMemcpyDeviceToHost)) != cudaSuccess) return LTLG_CUDA_ERROR;
     if (hc.status & (ST_WAIT | ST_TMA | ST_STALL)) return LTLG_DEVICE_WAIT;
-    if (hc.status & ST_TABLE) return LTLG_TABLE_FULL;
+    // a level that overflowed the scratch rows is the cause of anything after it
     if ((hc.status & ST_OVERFLOW) && !(hc.found && opt->stop_at_found)) return LTLG_NO_MEMORY;
+    if (hc.status & ST_TABLE) return LTLG_TABLE_FULL;
     const int last_cost = (int)hc.last_cost > c1 ? (int)hc.last_cost : c1;
 
     long long hls[MAX_COSTS + 3];

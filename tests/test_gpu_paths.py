@@ -86,12 +86,20 @@ def _relaxed_golden_runs():
 @pytest.mark.parametrize("run", _relaxed_golden_runs(), ids=lambda r: r["id"])
 def test_reference_keys_match_reference_runs(engine, run):
     """The reference's relaxed keys (types 1/2/3, lenSum > 126) on the device.  Of the CSs that
-    share a key in a level, the device keeps the one the reference's threads insert first
-    (blocks in order, thread order inside a block), as the oracle does: per-level sets of rows
-    and the per-block progress lines equal the oracle's exactly, in both schedules.  Against the
-    reference binary's own progress lines the rule of the oracle's pinning applies: cost 2 is
-    built from letters only and matches exactly, later stored counts within 1% (the reference
-    keeps whichever thread wins its atomic race).  The final cost is the reference's."""
+    share a key in a level, the device keeps the candidate first in the reference's order
+    (blocks in order, then thread index inside a block).  The per-block progress lines equal the
+    oracle's exactly.  Against the reference binary's own progress lines the rule of the
+    oracle's pinning applies: cost 2 is built from letters only and matches exactly, later
+    stored counts within 1% (the reference keeps whichever thread wins its atomic race).  The
+    final cost is the reference's.
+
+    Enumerated to max_cost, every stored row is its parents' operator applied to them, and each
+    level holds the oracle's number of rows with the oracle's set of keys while the levels below
+    hold the oracle's rows.  Which CS represents a shared key can differ: a thread index counts
+    rows of the operand levels in the order they were stored, and the device (like the
+    reference) stores a level's rows in the order its warps reach the hash set, while the oracle
+    stores them sequentially.  After the first level whose representatives differ, counts are
+    held to the 1% rule."""
     inst = load_fixture(run["file"])
     res = engine.learn(inst, costs=run["costs"], max_cost=run["max_cost"], neg_type=run["neg"],
                        key_mode=api.KEY_REF, rlx_type=run["rlx"], schedule=api.SCHEDULE_PER_BLOCK, limit_traces=True)
@@ -118,18 +126,31 @@ def test_reference_keys_match_reference_runs(engine, run):
     fused = engine.learn(inst, costs=run["costs"], max_cost=run["max_cost"], neg_type=run["neg"],
                          key_mode=api.KEY_REF, rlx_type=run["rlx"], limit_traces=True)
     assert (fused.status, fused.cost, fused.all_ltls) == (res.status, res.cost, res.all_ltls)
-    # every level's rows, enumerated to max_cost, are the oracle's representatives
+    # every level to max_cost
     full = engine.learn(inst, costs=run["costs"], max_cost=run["max_cost"], neg_type=run["neg"],
                         key_mode=api.KEY_REF, rlx_type=run["rlx"], limit_traces=True, stop_at_found=False)
+    assert full.device_flags & ~1 == 0
     want = O.learn(inst, costs=run["costs"], max_cost=run["max_cost"], neg_type=run["neg"], key_mode=run["rlx"],
                    limit_traces=True, stop_at_found=False)
     starts = engine.level_starts(run["max_cost"] + 2)
-    for c in range(run["costs"][0], run["max_cost"] + 1):
+    c1 = run["costs"][0]
+    rows, parents = engine.read_rows(0, starts[run["max_cost"] + 1])
+    mask = np.array([(1 << int(x)) - 1 for x in inst.lengths], dtype=np.uint64)
+    for i in range(starts[c1 + 1], len(rows)):  # each row is its parents' operator
+        p = int(parents[i])
+        op, left, right = (p >> 60) & 7, (p >> 30) & 0x3FFFFFFF, p & 0x3FFFFFFF
+        cs, _ = O.apply_op(op, rows[left], rows[right] if op in (1, 2, 6) else None, mask)
+        assert np.array_equal(cs, rows[i]), (i, op, left, right)
+    keys = lambda rs: {O.ref_key(np.ascontiguousarray(r), np.asarray(inst.lengths), run["rlx"]) for r in rs}
+    same_below = True
+    for c in range(c1, run["max_cost"] + 1):
         theirs = want.level_rows(c)
-        assert starts[c + 1] - starts[c] == len(theirs), c
-        if len(theirs):
-            rows, _ = engine.read_rows(starts[c], len(theirs))
-            assert row_set(rows) == row_set(theirs), c
+        mine = rows[starts[c]:starts[c + 1]]
+        if same_below:
+            assert len(mine) == len(theirs) and keys(mine) == keys(theirs), c
+            same_below = row_set(mine) == row_set(theirs)
+        else:
+            assert abs(len(mine) - len(theirs)) <= max(2, 0.01 * len(theirs)), (c, len(mine), len(theirs))
 
 
 @pytest.mark.parametrize("name", sorted(edge_cases()))

@@ -107,7 +107,7 @@ struct ltlg_engine {
     int n = 0, pitch = 0, nalpha = 0, max_cost = 0;
     long long cap_rows = 0;
     int tile = 0, stages = 0, grid = 0, hk = 0;
-    long long tile_bytes = 0, row_bytes = 0;
+    long long tile_bytes = 0;
     std::vector<long long> level_start;
     std::string last_error;
 };
@@ -198,20 +198,15 @@ void build_string(const std::map<u64, u64> &par, u64 row, u64 p, bool is_root, c
     }
 }
 
-// Level-kernel geometry for rows of `pitch` words.  Rows of at least STAGE_MIN_PITCH words are
-// staged per consumer warp when those buffers and three slots of 2-row tiles fit the shared
-// memory; the rest of the budget holds the slots' tiles: the left tile is shrunk from `want`
-// until at least three slots fit.  Returns false when not even one slot of a 2-row tile fits.
-bool geometry(int want, int pitch, int &tile, int &stages, long long &tile_bytes, long long &row_bytes) {
-    constexpr long long BUDGET = 216 * 1024;  // dynamic shared memory for tiles and staged rows
-    constexpr int STAGE_MIN_PITCH = 128;
-    const long long rb = (long long)pitch * 8;
-    row_bytes = pitch >= STAGE_MIN_PITCH && LEVEL_CONSUMERS * rb + 3 * 2 * rb <= BUDGET ? rb : 0;
-    const long long budget = BUDGET - LEVEL_CONSUMERS * row_bytes;
+// Level-kernel geometry for rows of `pitch` words: the left tile (shrunk from `want` until at
+// least three item slots fit the shared memory) and the slots.  Returns false when not even one
+// slot of a 2-row tile fits.
+bool geometry(int want, int pitch, int &tile, int &stages, long long &tile_bytes) {
+    constexpr long long BUDGET = 200 * 1024;  // dynamic shared memory for the slots' tiles
     tile = want;
-    while (tile > 2 && budget / ((long long)tile * rb) < 3) tile /= 2;
-    tile_bytes = (long long)tile * rb;
-    stages = (int)std::min<long long>(8, budget / tile_bytes);
+    while (tile > 2 && BUDGET / ((long long)tile * pitch * 8) < 3) tile /= 2;
+    tile_bytes = (long long)tile * pitch * 8;
+    stages = (int)std::min<long long>(8, BUDGET / tile_bytes);
     return stages >= 1;
 }
 
@@ -371,7 +366,6 @@ cudaError_t run_levels(ltlg_engine *e, bool persist, int grid, double t0, double
     hl->tile = e->tile;
     hl->stages = e->stages;
     hl->tile_bytes = e->tile_bytes;
-    hl->row_bytes = e->row_bytes;
     cudaStream_t st = e->stream;
     cudaError_t err = cudaMemcpyAsync(e->launch.p, hl, sizeof(Launch), cudaMemcpyHostToDevice, st);
     if (err != cudaSuccess) return err;
@@ -505,16 +499,15 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     }
     if (cap_rows < nalpha + 1) return fail_status(res, LTLG_NO_MEMORY);
     int tile = 0, stages = 0;
-    long long tile_bytes = 0, row_bytes = 0;
-    if (!geometry(e->cfg.left_tile, pitch, tile, stages, tile_bytes, row_bytes)) return fail_status(res, LTLG_BAD_ARGS);
+    long long tile_bytes = 0;
+    if (!geometry(e->cfg.left_tile, pitch, tile, stages, tile_bytes)) return fail_status(res, LTLG_BAD_ARGS);
     const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
-    const size_t smem = level_kernel_smem(stages, tile_bytes, row_bytes);
+    const size_t smem = level_kernel_smem(stages, tile_bytes);
     const int per_sm = level_kernel_ctas_per_sm(hk, smem);
     if (per_sm < 1) return fail_status(res, LTLG_BAD_ARGS);
     e->tile = tile;
     e->stages = stages;
     e->tile_bytes = tile_bytes;
-    e->row_bytes = row_bytes;
     e->hk = hk;
     e->grid = e->num_sms * per_sm;
 
@@ -1215,10 +1208,10 @@ LTLG_API int ltlg_batch_learn(ltlg_batch *b, const ltlg_traces *traces, int32_t 
         const bool keyed = opt->key_mode != LTLG_KEY_EXACT;
         const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
         int tile = 0, stages = 0;
-        long long tile_bytes = 0, row_bytes = 0;
-        if (!geometry(b->cfg.left_tile, max_pitch, tile, stages, tile_bytes, row_bytes)) err = cudaErrorInvalidValue;
+        long long tile_bytes = 0;
+        if (!geometry(b->cfg.left_tile, max_pitch, tile, stages, tile_bytes)) err = cudaErrorInvalidValue;
         const int per_sm =
-            err == cudaSuccess ? level_kernel_ctas_per_sm(hk, level_kernel_smem(stages, tile_bytes, row_bytes)) : 0;
+            err == cudaSuccess ? level_kernel_ctas_per_sm(hk, level_kernel_smem(stages, tile_bytes)) : 0;
         if (per_sm < 1 && err == cudaSuccess) err = cudaErrorInvalidConfiguration;
         const int grid = b->num_sms * std::max(per_sm, 1);
         // inputs: instance records, steps and offsets of every instance in one array each
@@ -1343,7 +1336,6 @@ LTLG_API int ltlg_batch_learn(ltlg_batch *b, const ltlg_traces *traces, int32_t 
             L.tile = tile;
             L.stages = stages;
             L.tile_bytes = tile_bytes;
-            L.row_bytes = row_bytes;
             cudaStream_t st = b->stream;
             err = cudaMemcpyAsync(b->bin.p, b->h_bin.p, (size_t)nd * sizeof(BatchIn), cudaMemcpyHostToDevice, st);
             if (err == cudaSuccess && total_steps)

@@ -73,6 +73,8 @@ struct Slot {
     int stop;                 // remaining rows are skipped (a find at or before this entry)
     int inst;                 // the item's instance (index into Launch::args)
     int trace_first;          // the producer's first item of this plan (level stamps)
+    int overflowed;           // the cache had overflowed when the item was claimed (or a claim here
+                              // overflowed): the rows' new CSs take no hash slots
     InstArgs args;            // its arguments as they were when the item was claimed (a batch slot's
                               // arguments change when it takes the next instance)
 };
@@ -80,14 +82,13 @@ struct Slot {
 // ---------------------------------------------------------------- candidate generators
 // pre(c) loads what every candidate of the set shares at chunk c (binary: the right row;
 // unary: the word metadata); word(t, c, pre) gives words 2c, 2c+1 of candidate t.
-// ST: the right (or source) row is staged in shared memory, else it is read from the cache.
-template <int OPC, bool ST>
+template <int OPC>
 struct BinGen {
     const ulonglong2 *left;   // shared-memory tile, row stride nch
-    const ulonglong2 *right;  // right row (shared memory when ST)
+    const ulonglong2 *right;  // global right row
     int nch;
     int rop;
-    __device__ __forceinline__ ulonglong2 pre(int c) const { return ST ? right[c] : __ldcg(right + c); }
+    __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldcg(right + c); }
     __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 r) const {
         if (OPC == OP_U) {
             const ulonglong2 l = left[(t >> 1) * nch + c];
@@ -101,13 +102,12 @@ struct BinGen {
 };
 
 // Candidate t of a fused unary row: operator slot t (0 ~, 1 X, 2 F, 3 G) of one source row.
-template <bool ST>
 struct UnGen {
-    const ulonglong2 *src;   // source row (shared memory when ST)
+    const ulonglong2 *src;
     const ulonglong2 *meta;
     __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldcg(meta + c); }
     __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 m) const {
-        const ulonglong2 s = ST ? src[c] : __ldcg(src + c);
+        const ulonglong2 s = __ldcg(src + c);
         const int op = unary_slot_op(t);
         return make_ulonglong2(unary_word(op, s.x, m.x & LENMASK), unary_word(op, s.y, m.y & LENMASK));
     }
@@ -229,7 +229,8 @@ __device__ void take_over(const InstArgs &A, InstCtl *C, const Gen &g, int t, u6
 
 template <int NC, class Gen>
 __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost, const Gen &g, u64 fp, bool active,
-                                        u64 parent, u64 kh, u64 kl, u64 prio, u32 anyp, u32 anyn, int lane) {
+                                        u64 parent, u64 kh, u64 kl, u64 prio, u32 anyp, u32 anyn, int *overflowed,
+                                        int lane) {
     int state = active ? S_PROBE : S_DONE;
     const u64 tagbits = (fp >> 40) << 40;
     const u64 genbits = (u64)A.gen << 32;
@@ -392,10 +393,6 @@ __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost,
 template <int NC, class Gen, class ParentOf, class PosOf, class TidOf>
 __device__ __forceinline__ void finish(const InstArgs &A, InstCtl *C, Slot &sl, const Gen &g, u64 (&h)[NC], u32 bp,
                                        u32 bn, u32 valid, ParentOf parent_of, PosOf pos_of, TidOf tid_of, int lane) {
-    // once the language cache has overflowed, the level's remaining CSs are not stored and take
-    // no hash slots (loaded first: its latency hides behind the reduction)
-    u32 st = 0;
-    if (lane == 0 && !sl.check_only) st = *(volatile const u32 *)&C->status;
     const u64 sum = reduce_to_lane<NC>(h, lane);
     const u32 anyp = __reduce_or_sync(FULL, bp), anyn = __reduce_or_sync(FULL, bn);
     const u32 acc = ~(anyp | anyn) & valid;
@@ -432,16 +429,18 @@ __device__ __forceinline__ void finish(const InstArgs &A, InstCtl *C, Slot &sl, 
         fp = fmix64(kh ^ fmix64(kl + 0x5ad0dedull));
     }
     const u64 prio = A.prio && ((valid >> lane) & 1u) ? ((u64)(u32)pos_of(lane) << 40) | tid_of(lane) : 0ull;
-    const bool room = (__shfl_sync(FULL, st, 0) & ST_OVERFLOW) == 0u;
-    resolve<NC>(A, C, cost, g, fp, room && ((valid >> lane) & 1u), myparent, kh, kl, prio, anyp, anyn, lane);
+    // once the language cache has overflowed, the level's remaining CSs are not stored and take
+    // no hash slots
+    const bool room = *(volatile int *)&sl.overflowed == 0;
+    resolve<NC>(A, C, cost, g, fp, room && ((valid >> lane) & 1u), myparent, kh, kl, prio, anyp, anyn, &sl.overflowed,
+                lane);
 }
 
 // ---------------------------------------------------------------- rows
-// Binary row: right row r (at R: in the cache, or the warp's staged copy with ST) against the
-// slot's tile of TLP left rows (U: both orders of each pair, TL = 2 TLP candidates; & and |:
-// TL = TLP).  Chunks are 16 bytes (two words); four are in flight per lane.  Positives are the
-// first npos words, so acceptance needs no metadata.
-template <int OPC, int TL, int HK, bool ST>
+// Binary row: right row r (at R) against the slot's tile of TLP left rows (U: both orders of
+// each pair, TL = 2 TLP candidates; & and |: TL = TLP).  Chunks are 16 bytes (two words); four
+// are in flight per lane.  Positives are the first npos words, so acceptance needs no metadata.
+template <int OPC, int TL, int HK>
 __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &sl, const ulonglong2 *tile,
                                            const ulonglong2 *R, long long r, int lane) {
     constexpr int TLP = OPC == OP_U ? TL / 2 : TL;
@@ -457,7 +456,7 @@ __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int c = c0 + 32 * u;
-            if (c < nch) rvv[u] = ST ? R[c] : __ldcg(R + c);
+            if (c < nch) rvv[u] = __ldcg(R + c);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -494,7 +493,7 @@ __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &
     }
     const int cnt = OPC == OP_U ? 2 * nl : nl;
     const u32 valid = cnt >= 32 ? FULL : ((1u << cnt) - 1u);
-    const BinGen<OPC, ST> g{tile, R, nch, rop};
+    const BinGen<OPC> g{tile, R, nch, rop};
     const long long l_first = sl.l_first;
     finish<NC>(A, C, sl, g, h, bp, bn, valid,
                [&](int t) {
@@ -514,9 +513,8 @@ __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &
     if (lane == 0) atomicAdd(&sl.evals, (unsigned)cnt);
 }
 
-// Unary row: every operator of the slot's mask on source row s (at src: in the cache, or the
-// warp's staged copy with ST; one load of each chunk).
-template <int HK, bool ST>
+// Unary row: every operator of the slot's mask on source row s (at src; one load of each chunk).
+template <int HK>
 __device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &sl, const ulonglong2 *src, long long s,
                                           int lane) {
     constexpr int NC = 4;
@@ -531,7 +529,7 @@ __device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &s
         for (int u = 0; u < 2; ++u) {
             const int c = c0 + 32 * u;
             if (c < nch) {
-                sv[u] = ST ? src[c] : __ldcg(src + c);
+                sv[u] = __ldcg(src + c);
                 mv[u] = __ldcg(meta + c);  // a batch slot rewrites its metadata in the launch
             }
         }
@@ -556,7 +554,7 @@ __device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &s
         }
     }
     const u32 valid = (u32)(mask & 15);
-    const UnGen<ST> g{src, meta};
+    const UnGen g{src, meta};
     finish<NC>(A, C, sl, g, h, bp, bn, valid,
                [&](int t) { return pack_parent(unary_slot_op(t & 3), (u64)s, 0); },
                [&](int t) { return sl.upos[t & 3]; }, [&](int) -> u64 { return (u64)(s - sl.e_r0); }, lane);
@@ -861,11 +859,10 @@ __device__ void score_plan(const InstArgs &A, InstCtl *C, int lane) {
 // windows first).  Lane 0.
 __device__ __forceinline__ void publish(InstCtl *C, long long items, bool open) {
     const u32 seq = __ldcg(&C->seq) + 1;
+    __threadfence();  // the plan and entries (written by the whole warp) come first
     C->done = 0;
-    __threadfence();
     C->limit = ((u64)seq << SEQ_SHIFT) | (u64)(open ? items : 0);
-    __threadfence();
-    st_release(&C->claimed, (u64)seq << SEQ_SHIFT);
+    st_release(&C->claimed, (u64)seq << SEQ_SHIFT);  // orders done and limit before the new sequence
     st_release32(&C->seq, seq);
 }
 
@@ -873,7 +870,7 @@ __device__ __forceinline__ void publish(InstCtl *C, long long items, bool open) 
 // stopping when the search is over.  Levels without any block are closed on the spot.  One
 // warp (all lanes).  With open false (host-driven levels) the next plan is made but hands out
 // nothing until the host opens it.
-__device__ __noinline__ bool close_level(const InstArgs &A, InstCtl *C, bool open, int lane) {
+__device__ bool close_level(const InstArgs &A, InstCtl *C, bool open, int lane) {
     __threadfence();
     int c = (int)__ldcg(&C->plan.cost);
     bool halt = false;
@@ -1313,7 +1310,7 @@ __device__ __forceinline__ bool launch_done(const Launch &L, int lane) {
 
 // The producer warp: claims items, fills slots, issues the tile copies and the L2 prefetches.
 template <int TL>
-__device__ __noinline__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int lane) {
+__device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int lane) {
     __shared__ ProdCache pc;
     const int S = L.stages;
     const long long tile_words = L.tile_bytes / 8;
@@ -1345,25 +1342,35 @@ __device__ __noinline__ void producer(const Launch &L, unsigned char *smem, u64 
         // advance the counter.
         long long item = -1;
         u64 tag = 0, fk = NO_FIND;
+        u32 ovf = 0;
         int tries = 0;
         u64 t_wait = 0, last_done = ~0ull;
         for (;;) {
             InstCtl *C = ctl_of(L, inst);
             u64 v = 0, lim = 0, f = NO_FIND;
+            u32 stt = 0;
             if (lane == 0) {
                 if (optimistic) {
                     lim = ld_volatile(&C->limit);
                     f = ld_volatile(&C->found_key);
+                    stt = *(volatile const u32 *)&C->status;
                     v = atomicAdd(&C->claimed, 1ull);
-                    if ((v >> SEQ_SHIFT) != (lim >> SEQ_SHIFT)) lim = ld_volatile(&C->limit);  // a newer plan
+                    if ((v >> SEQ_SHIFT) != (lim >> SEQ_SHIFT)) {  // a newer plan: its limit was released before it
+                        __threadfence();
+                        lim = ld_volatile(&C->limit);
+                    }
                 } else {
                     lim = ld_volatile(&C->limit);
                     const u64 cur = ld_volatile(&C->claimed);
                     v = cur;
                     if ((cur >> SEQ_SHIFT) == (lim >> SEQ_SHIFT) && cur < lim) {
                         f = ld_volatile(&C->found_key);
+                        stt = *(volatile const u32 *)&C->status;
                         v = atomicAdd(&C->claimed, 1ull);
-                        lim = ld_volatile(&C->limit);
+                        if ((v >> SEQ_SHIFT) != (lim >> SEQ_SHIFT)) {
+                            __threadfence();
+                            lim = ld_volatile(&C->limit);
+                        }
                     }
                 }
             }
@@ -1374,6 +1381,7 @@ __device__ __noinline__ void producer(const Launch &L, unsigned char *smem, u64 
                 item = (long long)(v & ITEM_MASK);
                 tag = v >> SEQ_SHIFT;
                 fk = f;
+                ovf = __shfl_sync(FULL, stt, 0) & ST_OVERFLOW;
                 optimistic = true;
                 break;
             }
@@ -1478,6 +1486,7 @@ __device__ __noinline__ void producer(const Launch &L, unsigned char *smem, u64 
             const u32 bytes = fill_slot(sl, inst, pc.e, item, L.tile, pc.rc, pc.ur, pc.cost, pc.check_only,
                                         pc.plan_items, skip, pc.a.pitch);
             sl.trace_first = pc.trace_first;
+            sl.overflowed = ovf ? 1 : 0;
             pc.trace_first = 0;
             if (!skip) {
                 const u64 pitch = (u64)pc.a.pitch;
@@ -1507,20 +1516,14 @@ __device__ __noinline__ void producer(const Launch &L, unsigned char *smem, u64 
     __syncwarp();
 }
 
-// The rows of one slot a consumer warp takes, until the slot has none left.  With ST every row
-// is first copied into the warp's own shared-memory buffer `wrow` (one bulk copy, mbarrier
-// `wbar`, phase *wph), so the candidate words of the row, of the claims and of the
-// verifications come from shared memory.  Returns SLOT_CLOSE when this warp finished the
-// level's last item, SLOT_FAIL after a copy that did not arrive, else SLOT_NEXT.  No calls: the
-// cold work (closing a level, a batch slot's next instance) is the caller's, so the row loop
-// keeps its registers.
-enum { SLOT_NEXT = 0, SLOT_CLOSE = 1, SLOT_FAIL = 2 };
-template <int TL, int HK, bool ST>
-__device__ __noinline__ int take_rows(Slot &sl, int kind, const ulonglong2 *tile, u64 *wrow, u64 *wbar, u32 *wph,
-                                      int lane) {
+// The rows of one slot a consumer warp takes, until the slot has none left.  Returns
+// SLOT_CLOSE when this warp finished the level's last item, else SLOT_NEXT; closing the level
+// (with the slot's arguments, before the slot is released) is the caller's.
+enum { SLOT_NEXT = 0, SLOT_CLOSE = 1 };
+template <int TL, int HK>
+__device__ __forceinline__ int take_rows(Slot &sl, int kind, const ulonglong2 *tile, int lane) {
     const InstArgs &A = sl.args;
     InstCtl *C = A.ctl;
-    bool fenced = false;
     int out = SLOT_NEXT;
     for (;;) {
         unsigned idx = 0;
@@ -1532,33 +1535,12 @@ __device__ __noinline__ int take_rows(Slot &sl, int kind, const ulonglong2 *tile
         if (!*(volatile int *)&sl.stop) {
             const long long r = sl.row0 + idx;
             const ulonglong2 *rp = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)r * A.pitch);
-            if (ST) {
-                bool ok = true;
-                if (lane == 0) {
-                    // rows of the finished levels were written through the generic proxy
-                    if (!fenced) fence_proxy_async_global();
-                    fence_proxy_async();  // the warp's reads of the previous staged row come first
-                    const u32 bytes = (u32)A.pitch * 8u;
-                    mbar_expect_tx(wbar, bytes);
-                    bulk_g2s(wrow, rp, bytes, wbar);
-                    ok = mbar_wait_for(wbar, *wph, PIPE_WAIT_NS);
-                    if (!ok) {
-                        atomicOr(&C->status, ST_TMA);
-                        mbar_wait_for(wbar, *wph, PIPE_WAIT_NS);  // the copy in flight, before leaving
-                    }
-                }
-                fenced = true;
-                *wph ^= 1u;
-                if (!__shfl_sync(FULL, ok, 0)) return SLOT_FAIL;
-                rp = reinterpret_cast<const ulonglong2 *>(wrow);
-            }
             if (kind == ENT_UNARY)
-                unary_row<HK, ST>(A, C, sl, rp, r, lane);
+                unary_row<HK>(A, C, sl, rp, r, lane);
             else if (kind == ENT_ANDOR)
-                binary_row<OP_ANDOR_CLASS, TL, HK, ST>(A, C, sl, tile, rp, r, lane);
+                binary_row<OP_ANDOR_CLASS, TL, HK>(A, C, sl, tile, rp, r, lane);
             else
-                binary_row<OP_U, TL, HK, ST>(A, C, sl, tile, rp, r, lane);
-            if (ST) __syncwarp();  // every lane is done with the staged row before the next copy
+                binary_row<OP_U, TL, HK>(A, C, sl, tile, rp, r, lane);
         }
         unsigned d = 0;
         __threadfence_block();  // this row's evals count is in before the row counts as done
@@ -1581,12 +1563,10 @@ __device__ __noinline__ int take_rows(Slot &sl, int kind, const ulonglong2 *tile
 
 // A consumer warp: takes the rows of the slots in order until the producer's end slot; the
 // warp that finishes a level's last item closes the level (and plans the next one).
-template <int TL, int HK, bool ST>
-__device__ __noinline__ void consumer(const Launch &L, unsigned char *smem, const u64 *tiles, u64 *wrow, u64 *wbar,
-                                      int lane) {
+template <int TL, int HK>
+__device__ void consumer(const Launch &L, unsigned char *smem, const u64 *tiles, int lane) {
     const int S = L.stages;
     const long long tile_words = L.tile_bytes / 8;
-    u32 wph = 0;  // phase of wbar
     for (u64 k = 0;; ++k) {
         const int s = (int)(k % (u64)S);
         Slot &sl = *slot_at(smem, s);
@@ -1600,8 +1580,7 @@ __device__ __noinline__ void consumer(const Launch &L, unsigned char *smem, cons
         const int kind = *(volatile int *)&sl.kind;
         if (kind == 0) return;
         const ulonglong2 *tile = reinterpret_cast<const ulonglong2 *>(tiles + (u64)s * tile_words);
-        const int got = take_rows<TL, HK, ST>(sl, kind, tile, wrow, wbar, &wph, lane);
-        if (got == SLOT_FAIL) return;
+        const int got = take_rows<TL, HK>(sl, kind, tile, lane);
         int recycle = -1;  // a batch slot whose instance's search ended in this warp
         if (got == SLOT_CLOSE) {  // the slot's arguments are read before the slot is released
             const bool ended = close_level(sl.args, sl.args.ctl, L.persist != 0, lane);
@@ -1620,11 +1599,10 @@ namespace {
 
 __device__ __forceinline__ size_t slots_bytes(int S) { return ((size_t)S * sizeof(Slot) + 127) & ~(size_t)127; }
 
-template <int TL, int HK, bool ST>
+template <int TL, int HK>
 __global__ void __launch_bounds__(LEVEL_THREADS, 1) level_kernel(const Launch *__restrict__ Lp) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ Launch L;
-    __shared__ __align__(8) u64 wbar[NCONS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         L = *Lp;
@@ -1633,18 +1611,14 @@ __global__ void __launch_bounds__(LEVEL_THREADS, 1) level_kernel(const Launch *_
             mbar_init(&sl.full, 1);
             mbar_init(&sl.empty, NCONS);
         }
-        if (ST)
-            for (int w = 0; w < NCONS; ++w) mbar_init(&wbar[w], 1);
         fence_mbar_init();
     }
     __syncthreads();
     u64 *tiles = reinterpret_cast<u64 *>(smem + slots_bytes(L.stages));
-    if (warp == 0) {
+    if (warp == 0)
         producer<TL>(L, smem, tiles, lane);
-    } else {
-        u64 *rows = tiles + (u64)L.stages * (u64)(L.tile_bytes / 8);
-        consumer<TL, HK, ST>(L, smem, tiles, rows + (u64)(warp - 1) * (u64)(L.row_bytes / 8), &wbar[warp - 1], lane);
-    }
+    else
+        consumer<TL, HK>(L, smem, tiles, lane);
 }
 
 // A batch's first instances: block s sets slot s up (one warp per slot).
@@ -1874,7 +1848,7 @@ __global__ void eval_formula_kernel(const int *__restrict__ prog, int len, const
 
 // The dynamic shared-memory limit is a per-device function attribute: each device keeps the
 // largest size enabled on it so far.
-template <int TL, int HK, bool ST>
+template <int TL, int HK>
 cudaError_t smem_attr(size_t smem) {
     constexpr int MAX_DEVICES = 64;
     static std::atomic<long long> attr_set[MAX_DEVICES];
@@ -1883,7 +1857,7 @@ cudaError_t smem_attr(size_t smem) {
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev >= 0 && dev < MAX_DEVICES && (long long)smem <= attr_set[dev].load()) return cudaSuccess;
-    e = cudaFuncSetAttribute(level_kernel<TL, HK, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(level_kernel<TL, HK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess && dev >= 0 && dev < MAX_DEVICES) {
         long long cur = attr_set[dev].load();
         while (cur < (long long)smem && !attr_set[dev].compare_exchange_weak(cur, (long long)smem)) {
@@ -1892,48 +1866,45 @@ cudaError_t smem_attr(size_t smem) {
     return e;
 }
 
-template <int TL, int HK, bool ST>
+template <int TL, int HK>
 cudaError_t launch_tl(const Launch &h, const Launch *d, int grid, cudaStream_t s) {
-    const size_t smem = level_kernel_smem(h.stages, h.tile_bytes, h.row_bytes);
-    cudaError_t e = smem_attr<TL, HK, ST>(smem);
+    const size_t smem = level_kernel_smem(h.stages, h.tile_bytes);
+    cudaError_t e = smem_attr<TL, HK>(smem);
     if (e != cudaSuccess) return e;
-    level_kernel<TL, HK, ST><<<grid, LEVEL_THREADS, smem, s>>>(d);
+    level_kernel<TL, HK><<<grid, LEVEL_THREADS, smem, s>>>(d);
     return cudaGetLastError();
 }
 
-template <int TL, int HK, bool ST>
+template <int TL, int HK>
 int occupancy_tl(size_t smem) {
-    if (smem_attr<TL, HK, ST>(smem) != cudaSuccess) return 0;
+    if (smem_attr<TL, HK>(smem) != cudaSuccess) return 0;
     int n = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<TL, HK, ST>, LEVEL_THREADS, smem) ==
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, level_kernel<TL, HK>, LEVEL_THREADS, smem) ==
                    cudaSuccess
                ? n
                : 0;
 }
 
-template <int HK, bool ST>
+template <int HK>
 cudaError_t launch_hk(const Launch &h, const Launch *d, int grid, cudaStream_t s) {
-    return h.tile == 2   ? launch_tl<2, HK, ST>(h, d, grid, s)
-           : h.tile == 4 ? launch_tl<4, HK, ST>(h, d, grid, s)
-                         : launch_tl<8, HK, ST>(h, d, grid, s);
+    return h.tile == 2   ? launch_tl<2, HK>(h, d, grid, s)
+           : h.tile == 4 ? launch_tl<4, HK>(h, d, grid, s)
+                         : launch_tl<8, HK>(h, d, grid, s);
 }
 
 }  // namespace
 
-size_t level_kernel_smem(int stages, long long tile_bytes, long long row_bytes) {
-    return (((size_t)stages * sizeof(Slot) + 127) & ~(size_t)127) + (size_t)stages * (size_t)tile_bytes +
-           (size_t)NCONS * (size_t)row_bytes;
+size_t level_kernel_smem(int stages, long long tile_bytes) {
+    return (((size_t)stages * sizeof(Slot) + 127) & ~(size_t)127) + (size_t)stages * (size_t)tile_bytes;
 }
 
 cudaError_t launch_levels(const Launch &h, const Launch *d, int grid, int hk, cudaStream_t s) {
-    const bool st = h.row_bytes > 0;
-    if (hk == 1) return st ? launch_hk<1, true>(h, d, grid, s) : launch_hk<1, false>(h, d, grid, s);
-    return st ? launch_hk<0, true>(h, d, grid, s) : launch_hk<0, false>(h, d, grid, s);
+    return hk == 1 ? launch_hk<1>(h, d, grid, s) : launch_hk<0>(h, d, grid, s);
 }
 
 int level_kernel_ctas_per_sm(int hk, size_t smem) {
     // every tile instance has the same resource use up to its registers; ask the 8-row one
-    return hk == 1 ? occupancy_tl<8, 1, true>(smem) : occupancy_tl<8, 0, true>(smem);
+    return hk == 1 ? occupancy_tl<8, 1>(smem) : occupancy_tl<8, 0>(smem);
 }
 
 cudaError_t launch_first_plan(const InstArgs *d, int ninst, int open, cudaStream_t s) {

@@ -86,19 +86,22 @@ struct Plan {
     u64 cand;            // candidates of the level, counted as the reference counts them
 };
 
-// The mutable state of one instance's learn (device memory).
-struct InstCtl {
+// The mutable state of one instance's learn (device memory).  The words that many SMs touch
+// during a level sit in separate 128-byte lines, so the L2 serves them in parallel: the claim
+// line (producers: claim counter, limit, find key, status), the completion line (items done,
+// candidates evaluated) and the row line (row reservations).
+struct alignas(128) InstCtl {
     u64 claimed;         // plan sequence << SEQ_SHIFT | next queue item
     u64 limit;           // plan sequence << SEQ_SHIFT | end of the items handed out (the plan's items, or a window's end)
-    u64 done;            // items of the current plan (or window) finished; the level (window) ends at limit's item
-    u64 row_count;       // rows handed out, letters included (may pass cap_rows on overflow)
     u64 found_key;       // smallest (cost << 32 | block position) of an accepting candidate; NO_FIND
-    u64 found;           // (1 << 63) | parents of the find, once the level of the find has ended
-    u64 evaluated;       // candidates evaluated
     u32 status;          // ST_* bits
+    u32 seq;             // plans published (the current plan is sequence seq)
+    alignas(128) u64 done;  // items of the current plan (or window) finished; the level (window) ends at limit's item
+    u64 evaluated;       // candidates evaluated
+    alignas(128) u64 row_count;  // rows handed out, letters included (may pass cap_rows on overflow)
+    alignas(128) u64 found;      // (1 << 63) | parents of the find, once the level of the find has ended
     u32 found_cost;      // level of `found`
     u32 overflow_cost;   // level at which the cache first overflowed (0: none)
-    u32 seq;             // plans published (the current plan is sequence seq)
     u32 ne_count;        // non-empty levels so far (InstArgs::ne)
     u32 last_cost;       // the last level that ran to its end
     u32 flags;           // CTL_* bits
@@ -223,8 +226,6 @@ struct Launch {
     int tile;                // left rows staged per binary item (U: tile / 2 left rows, two candidates each)
     int stages;              // item slots in flight per CTA
     long long tile_bytes;    // shared-memory bytes of one slot's tile
-    long long row_bytes;     // > 0: every consumer warp copies the right (unary: source) row of each
-                             // candidate set into its own shared-memory buffer of this size first
 };
 
 // The feature inputs of a block (operator op) of level c: the same code on the device
@@ -261,9 +262,8 @@ __host__ __device__ inline BlockInfo block_info(int op, int c, int lcost, long l
 // Threads per CTA of the level kernel (one producer warp and the consumer warps).
 constexpr int LEVEL_THREADS = 512;
 constexpr int LEVEL_CONSUMERS = LEVEL_THREADS / 32 - 1;
-// Shared memory of one CTA of the level kernel: `stages` slots of tile_bytes each, and (row_bytes
-// > 0) one staged row per consumer warp.
-size_t level_kernel_smem(int stages, long long tile_bytes, long long row_bytes);
+// Shared memory of one CTA of the level kernel for `stages` slots of tile_bytes each.
+size_t level_kernel_smem(int stages, long long tile_bytes);
 
 // Launch wrappers (learn.cu).  The kernels read their arguments from device memory, so a
 // launch (or a captured graph) stays valid while the arguments change between learns.

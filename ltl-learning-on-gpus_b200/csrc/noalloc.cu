@@ -235,7 +235,7 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     const int hk = opt->key_mode == LTLG_KEY_HASH64 ? 1 : 0;
     int num_sms = 0;
     cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
-    const int per_sm = level_kernel_ctas_per_sm(hk, level_kernel_smem(stages, tile_bytes, 0));
+    const int per_sm = level_kernel_ctas_per_sm(hk, level_kernel_smem(stages, tile_bytes));
     const int grid = (num_sms > 0 ? num_sms : 1) * (per_sm > 0 ? per_sm : 1);
 
     // Inputs and zeroed state (default stream, synchronous copies from stack arrays).
@@ -301,7 +301,6 @@ extern "C" LTLG_API int ltlg_learn_noalloc(const ltlg_traces *t, const ltlg_opti
     L.tile = tile;
     L.stages = stages;
     L.tile_bytes = tile_bytes;
-    L.row_bytes = 0;  // rows of at most 64 words: read in place
     if ((err = cudaMemcpy(dargs, &A, sizeof(A), cudaMemcpyHostToDevice)) != cudaSuccess ||
         (err = cudaMemcpy(dlaunch, &L, sizeof(L), cudaMemcpyHostToDevice)) != cudaSuccess)
         return LTLG_CUDA_ERROR;

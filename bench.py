@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--right-chunk", type=int, default=16, help="large levels: right rows per binary item")
     ap.add_argument("--unary-rows", type=int, default=32, help="large levels: source rows per unary item")
     ap.add_argument("--left-tile", type=int, default=4, help="left rows staged in shared memory per binary item")
-    ap.add_argument("--block-threads", type=int, default=256)
+    ap.add_argument("--block-threads", type=int, default=1024, help="kept for the engine config layout (the level kernel runs 1024 threads per CTA)")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")

@@ -89,8 +89,8 @@ typedef struct ltlg_engine_config {
     int64_t cache_bytes;       /* language-cache budget in bytes (rows = budget / (8 * pitch)) */
     int64_t max_rows;          /* upper bound on cache rows (<= 2^30); 0 = budget only */
     int32_t max_traces;        /* largest n the engine accepts */
-    int32_t block_threads;     /* kept for the layout; the level kernel runs one CTA of 512 threads
-                                  per SM (a producer warp and 15 consumer warps) */
+    int32_t block_threads;     /* kept for the layout; the level kernel runs one CTA of 1024 threads
+                                  per SM (a producer warp and 31 consumer warps) */
     int32_t left_tile;         /* left rows staged in shared memory per binary work item: 2, 4 or 8 */
     int32_t right_chunk;       /* right rows per binary work item of a large level */
     int32_t unary_rows;        /* source rows per unary work item of a large level */
@@ -166,7 +166,7 @@ typedef struct ltlg_result {
 
 typedef struct ltlg_engine ltlg_engine;
 
-/* Defaults: device 0, 2^27 slots, 16 GiB cache, n <= 8192, 512 threads, left tile 4,
+/* Defaults: device 0, 2^27 slots, 16 GiB cache, n <= 8192, 1024 threads, left tile 4,
    right chunk 16, unary rows 32, small rows 1, default wait bound and small-level size. */
 LTLG_API void ltlg_default_engine_config(ltlg_engine_config *cfg);
 /* The reference's defaults: unit costs, maxCost 500, type 3, NegType 2, exact keys, fused, plain. */

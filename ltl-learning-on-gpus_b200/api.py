@@ -223,7 +223,7 @@ class Engine:
     """Device state for repeated learns: language cache, hash set, stream."""
 
     def __init__(self, device=0, slots_log2=27, cache_bytes=16 << 30, max_rows=64 << 20, max_traces=8192,
-                 block_threads=512, left_tile=4, right_chunk=16, unary_rows=32, small_rows=1, wait_spins=0,
+                 block_threads=1024, left_tile=4, right_chunk=16, unary_rows=32, small_rows=1, wait_spins=0,
                  small_level=0):
         L = lib()
         cfg = _engine_config(device, slots_log2, cache_bytes, max_rows, max_traces, block_threads, left_tile,
@@ -327,7 +327,7 @@ class Engine:
 
 
 def _engine_config(device=0, slots_log2=27, cache_bytes=16 << 30, max_rows=64 << 20, max_traces=8192,
-                   block_threads=512, left_tile=4, right_chunk=16, unary_rows=32, small_rows=1, wait_spins=0,
+                   block_threads=1024, left_tile=4, right_chunk=16, unary_rows=32, small_rows=1, wait_spins=0,
                    small_level=0) -> EngineConfig:
     cfg = EngineConfig()
     lib().ltlg_default_engine_config(C.byref(cfg))

@@ -292,7 +292,7 @@ __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost,
             if (lane == leader) base = atomicAdd(&C->row_count, (u64)__popc(cm));
             base = __shfl_sync(FULL, base, leader);
             const u64 cap = (u64)A.cap_rows;
-#pragma unroll 2
+#pragma unroll 1
             for (int c = lane; c < nch; c += 32) {
                 const ulonglong2 p = g.pre(c);
 #pragma unroll
@@ -353,7 +353,7 @@ __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost,
 #pragma unroll
                 for (int t = 0; t < NC; ++t)
                     vr[t] = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)__shfl_sync(FULL, myv, t) * pitch);
-#pragma unroll 4
+#pragma unroll 1
                 for (int c = lane; c < nch; c += 32) {
                     const ulonglong2 p = g.pre(c);
 #pragma unroll
@@ -438,7 +438,7 @@ __device__ __forceinline__ void finish(const InstArgs &A, InstCtl *C, Slot &sl, 
 
 // ---------------------------------------------------------------- rows
 // Binary row: right row r (at R) against the slot's tile of TLP left rows (U: both orders of
-// each pair, TL = 2 TLP candidates; & and |: TL = TLP).  Chunks are 16 bytes (two words); four
+// each pair, TL = 2 TLP candidates; & and |: TL = TLP).  Chunks are 16 bytes (two words); two
 // are in flight per lane.  Positives are the first npos words, so acceptance needs no metadata.
 template <int OPC, int TL, int HK>
 __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &sl, const ulonglong2 *tile,
@@ -451,15 +451,15 @@ __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &
 #pragma unroll
     for (int t = 0; t < NC; ++t) h[t] = 0;
     u32 bp = 0, bn = 0;
-    for (int c0 = lane; c0 < nch; c0 += 128) {
-        ulonglong2 rvv[4];
+    for (int c0 = lane; c0 < nch; c0 += 64) {
+        ulonglong2 rvv[2];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < 2; ++u) {
             const int c = c0 + 32 * u;
             if (c < nch) rvv[u] = __ldcg(R + c);
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < 2; ++u) {
             const int c = c0 + 32 * u;
             if (c >= nch) continue;
             const u64 k = (2ull * (u64)c + 1ull) * WEYL;

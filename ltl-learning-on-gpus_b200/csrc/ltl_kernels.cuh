@@ -260,7 +260,7 @@ __host__ __device__ inline BlockInfo block_info(int op, int c, int lcost, long l
 }
 
 // Threads per CTA of the level kernel (one producer warp and the consumer warps).
-constexpr int LEVEL_THREADS = 512;
+constexpr int LEVEL_THREADS = 1024;
 constexpr int LEVEL_CONSUMERS = LEVEL_THREADS / 32 - 1;
 // Shared memory of one CTA of the level kernel for `stages` slots of tile_bytes each.
 size_t level_kernel_smem(int stages, long long tile_bytes);

@@ -78,3 +78,20 @@ def test_batch_host_paths():
         for inst, r in zip([small, deep], rel):
             w = e.learn(inst, neg_type=1, key_mode=api.KEY_REF, rlx_type=3, max_cost=6)
             assert (r.status, r.cost) == (w.status, w.cost)
+
+
+def test_cfg4_sample_matches_oracle():
+    """The first 256 instances of the cfg4 batch (2-4 propositions, 8-256 positive and negative
+    traces of length 4-40, hidden formula size 3-8, unit costs) in one batch launch with the
+    autotuner's kind of configuration: every minimal cost and candidate count is the oracle's,
+    and every formula separates its traces at that cost."""
+    from ltlb200 import workloads
+    insts = [gen.generate(*s) for s in workloads.cfg4_specs(4096, 0)[:256]]
+    with api.Batch(workers=16, slots_log2=22, cache_bytes=1 << 30, max_traces=512, left_tile=4, right_chunk=32,
+                   unary_rows=16) as pool:
+        res = pool.learn(insts, neg_type=1)
+    for inst, r in zip(insts, res):
+        want = O.learn(inst, neg_type=1, threads=0, keep_rows=False, cache_rows=1 << 21)
+        assert r.status == api.FOUND and want.status == O.FOUND
+        assert (r.cost, r.all_ltls) == (want.cost, want.all_ltls)
+        assert O.separates(r.formula, inst) and O.formula_cost(r.formula) == r.cost

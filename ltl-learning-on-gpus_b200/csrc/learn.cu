@@ -1474,8 +1474,16 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
             __syncwarp();
         }
         // skip rule: a find at or before this entry's block (or any find, find_first) in this level
-        const bool skip = pc.a.stop_at_found && fk != NO_FIND && (int)(fk >> 32) == pc.cost &&
-                          (pc.a.find_first || pc.e.pos >= (int)(u32)fk);
+        const bool found_here = pc.a.stop_at_found && fk != NO_FIND && (int)(fk >> 32) == pc.cost;
+        const bool skip = found_here && (pc.a.find_first || pc.e.pos >= (int)(u32)fk);
+        // the same rule for the items of this level still in this CTA's slots: their remaining
+        // rows are skipped (the slot the producer is about to fill is not in flight)
+        if (found_here && lane < S && lane != s) {
+            Slot &o = *slot_at(smem, lane);
+            if (*(volatile int *)&o.kind != 0 && o.inst == inst && o.cost == pc.cost &&
+                (pc.a.find_first || o.pos >= (int)(u32)fk))
+                *(volatile int *)&o.stop = 1;
+        }
         {
             constexpr int AW = sizeof(InstArgs) / 8;
             for (int w = lane; w < AW; w += 32)

@@ -233,10 +233,13 @@ def learned_order_report(ekw, repeats: int = 2):
         "time_to_minimal_ms": {"plain": s["ms_plain"], "learned": s["ms_learned"]},
         "speedup": s["speedup"],
         "device_ms": {"plain": s["device_ms_plain"], "learned": s["device_ms_learned"]},
+        "device_speedup": s["device_speedup"],
         "candidates_before_find": {"plain": s["evaluated_plain"], "learned": s["evaluated_learned"]},
         "cost_ge_8": {"instances": len(hard),
                       "speedup_total_time": (sum(r["ms_plain"] for r in hard) / max(1e-9, sum(r["ms_learned"] for r in hard)))
-                      if hard else None},
+                      if hard else None,
+                      "device_speedup": (sum(r["dev_ms_plain"] for r in hard) /
+                                         max(1e-9, sum(r["dev_ms_learned"] for r in hard))) if hard else None},
         "per_instance": [[r["cost_plain"], round(r["ms_plain"], 3), round(r["ms_learned"], 3)] for r in rows],
         "scorer": "scorer_hamming.npy: MLP 32-64-64-1, BF16/FP32, trained on the GPU on 198,070 block records",
         "spec_shape": near_miss_report(ekw),

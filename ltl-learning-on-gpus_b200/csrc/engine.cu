@@ -640,7 +640,8 @@ LTLG_API int ltlg_engine_learn(ltlg_engine *e, const ltlg_traces *t, const ltlg_
     A.found_par = (u64 *)e->fpar.p;
     A.ctl = (InstCtl *)e->ctl.p;
     A.model = learned ? e->scorer.p : nullptr;
-    A.cancel = (const volatile u32 *)e->cancel_dev;
+    // the planner reads the (mapped host) cancel flag at each level end only under a time limit
+    A.cancel = opt->time_limit_s > 0 ? (const volatile u32 *)e->cancel_dev : nullptr;
     const InstArgs *dA = (const InstArgs *)e->args.p;
     cudaMemcpyAsync(e->args.p, ha, sizeof(InstArgs), cudaMemcpyHostToDevice, st);
     if ((err = launch_insert_letters(dA, nalpha, hk, st)) != cudaSuccess) return fail_cuda(e, err, res);

@@ -47,6 +47,7 @@ constexpr int ENTRY_CACHE = 256;               // item starts of a plan's first 
 constexpr int NWARPS = LEVEL_THREADS / 32;
 constexpr int NCONS = NWARPS - 1;              // consumer warps per CTA
 static_assert(NCONS == LEVEL_CONSUMERS, "consumer warps");
+
 constexpr u64 PIPE_WAIT_NS = 30000000000ull;   // a consumer's wait for the producer (beyond every producer bound)
 constexpr u64 EMPTY_WAIT_NS = 10000000000ull;  // the producer's wait for the consumers to leave a slot
 constexpr u64 STALL_NS = 4000000000ull;        // no level progress while waiting for the next plan
@@ -451,15 +452,16 @@ __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &
 #pragma unroll
     for (int t = 0; t < NC; ++t) h[t] = 0;
     u32 bp = 0, bn = 0;
-    for (int c0 = lane; c0 < nch; c0 += 64) {
-        ulonglong2 rvv[2];
+    constexpr int CH = 2;  // right-row chunks in flight per lane
+    for (int c0 = lane; c0 < nch; c0 += 32 * CH) {
+        ulonglong2 rvv[CH];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < CH; ++u) {
             const int c = c0 + 32 * u;
             if (c < nch) rvv[u] = __ldcg(R + c);
         }
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < CH; ++u) {
             const int c = c0 + 32 * u;
             if (c >= nch) continue;
             const u64 k = (2ull * (u64)c + 1ull) * WEYL;
@@ -523,10 +525,11 @@ __device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &s
     const ulonglong2 *meta = reinterpret_cast<const ulonglong2 *>(A.wmeta);
     u64 h[NC] = {0, 0, 0, 0};
     u32 bp = 0, bn = 0;
-    for (int c0 = lane; c0 < nch; c0 += 64) {
-        ulonglong2 sv[2], mv[2];
+    constexpr int CH = 2;  // source-row chunks in flight per lane
+    for (int c0 = lane; c0 < nch; c0 += 32 * CH) {
+        ulonglong2 sv[CH], mv[CH];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < CH; ++u) {
             const int c = c0 + 32 * u;
             if (c < nch) {
                 sv[u] = __ldcg(src + c);
@@ -534,7 +537,7 @@ __device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &s
             }
         }
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < CH; ++u) {
             const int c = c0 + 32 * u;
             if (c >= nch) continue;
             const u64 k = (2ull * (u64)c + 1ull) * WEYL;
@@ -584,15 +587,15 @@ __device__ __forceinline__ void store_entry(Entry *dst, const Entry &e) {
 // The binary blocks of operator op (cost cop) of level c, in the reference's split order
 // (i = c1 .. (c - cop) / 2 over non-empty levels i and j = c - i - cop): written as entries
 // from queue index *eidx and positions from *pos.  Returns the candidates of this lane's blocks.
-__device__ u64 plan_binary(const InstArgs &A, int c, int op, int ne_count, int &pos, int &eidx, u64 &units,
-                           int lane) {
+__device__ u64 plan_binary(const InstArgs &A, int c, int op, int ne_count, int ne_lane, int &pos, int &eidx,
+                           u64 &units, int lane) {
     const int cop = A.cf[op + 1], c1 = A.cf[0];
     const int tl = op == OP_U ? max(1, A.tile / 2) : A.tile;
     u64 cand = 0;
     if (c - cop < 2 * c1) return 0;
     for (int base = 0; base < ne_count; base += 32) {
         const int q = base + lane;
-        const int i = q < ne_count ? __ldcg(A.ne + q) : 0;
+        const int i = q < ne_count ? (base == 0 ? ne_lane : __ldcg(A.ne + q)) : 0;
         const bool ok_i = q < ne_count && i >= c1 && 2 * i <= c - cop;
         long long li = 0, hi_ = 0, lj = 0, hj = 0;
         if (ok_i) {
@@ -633,6 +636,9 @@ __device__ u64 plan_binary(const InstArgs &A, int c, int op, int ne_count, int &
 __device__ void plan_level(const InstArgs &A, InstCtl *C, int c, int lane) {
     const int c1 = A.cf[0];
     const int ne_count = (int)__ldcg(&C->ne_count);
+    const u64 found_key = __ldcg(&C->found_key);  // loaded early: nothing changes it while planning
+    // the first 32 non-empty levels, one per lane, for all three binary operators
+    const int ne_lane = lane < ne_count ? __ldcg(A.ne + lane) : 0;
     // unary operators: lane j < 4 looks at slot operator j
     bool uex = false;
     long long ulo = 0, uhi = 0;
@@ -669,11 +675,11 @@ __device__ void plan_level(const InstArgs &A, InstCtl *C, int c, int lane) {
     int upos[4] = {POS_NONE, POS_NONE, POS_NONE, POS_NONE};
     if (um & 1u) upos[0] = pos++;
     u64 units_b = 0, units_u = 0;  // binary: (left tile, right row) pairs; unary: source rows
-    u64 cand = plan_binary(A, c, OP_AND, ne_count, pos, eidx, units_b, lane);
-    cand += plan_binary(A, c, OP_OR, ne_count, pos, eidx, units_b, lane);
+    u64 cand = plan_binary(A, c, OP_AND, ne_count, ne_lane, pos, eidx, units_b, lane);
+    cand += plan_binary(A, c, OP_OR, ne_count, ne_lane, pos, eidx, units_b, lane);
     for (int j = 1; j < 4; ++j)
         if ((um >> j) & 1u) upos[j] = pos++;
-    cand += plan_binary(A, c, OP_U, ne_count, pos, eidx, units_b, lane);
+    cand += plan_binary(A, c, OP_U, ne_count, ne_lane, pos, eidx, units_b, lane);
     if (lane == 0) {
         for (int g = 0; g < nu; ++g) {
             Entry e{};
@@ -745,7 +751,7 @@ __device__ void plan_level(const InstArgs &A, InstCtl *C, int c, int lane) {
         items += __shfl_sync(FULL, incl, 31);
     }
     // the find record of the level's blocks starts empty (unless an earlier level holds the find)
-    if (__ldcg(&C->found_key) == NO_FIND)
+    if (found_key == NO_FIND)
         for (int p = lane; p < nblocks; p += 32) __stcg(A.found_par + p, 0ull);
     if (lane == 0) {
         Plan &P = C->plan;

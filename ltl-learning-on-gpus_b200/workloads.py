@@ -143,7 +143,7 @@ AUTOTUNE_SPACE = [dict(left_tile=lt, right_chunk=rc, unary_rows=ur, slots_log2=s
                   for lt in (4, 8) for rc in (8, 32) for ur in (16, 64) for sl in (20, 22) for w in (48, 96)]
 
 
-def autotune(sample, space=AUTOTUNE_SPACE, cache_bytes=1 << 30, repeats=2, device=0, **opts):
+def autotune(sample, space=AUTOTUNE_SPACE, cache_bytes=1 << 30, repeats=3, device=0, **opts):
     """Time the batch call on `sample` under every configuration of `space` (tile shapes,
     item sizes, hash-set size = load factor, instance slots) and return (best, table)."""
     table = []
@@ -163,7 +163,7 @@ def autotune(sample, space=AUTOTUNE_SPACE, cache_bytes=1 << 30, repeats=2, devic
     return min(good, key=lambda t: t["seconds"]), table
 
 
-def run_cfg4(count=4096, seed=0, tune_sample=256, gen_workers=16, device=0) -> dict:
+def run_cfg4(count=4096, seed=0, tune_sample=1024, gen_workers=16, device=0) -> dict:
     """Generate the cfg4 batch, autotune the engine configuration on a sample, learn the whole
     batch with the best one; instances/s, unique CS/s, time to minimal formula."""
     t0 = time.perf_counter()

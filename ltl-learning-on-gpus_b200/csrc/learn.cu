@@ -47,6 +47,7 @@ constexpr int ENTRY_CACHE = 256;               // item starts of a plan's first 
 constexpr int NWARPS = LEVEL_THREADS / 32;
 constexpr int NCONS = NWARPS - 1;              // consumer warps per CTA
 static_assert(NCONS == LEVEL_CONSUMERS, "consumer warps");
+constexpr int WU = 1;  // chunks per lane loaded per round of a claim's write sweep (2 and 4 measured slower)
 
 constexpr u64 PIPE_WAIT_NS = 30000000000ull;   // a consumer's wait for the producer (beyond every producer bound)
 constexpr u64 EMPTY_WAIT_NS = 10000000000ull;  // the producer's wait for the consumers to leave a slot
@@ -81,15 +82,18 @@ struct Slot {
 };
 
 // ---------------------------------------------------------------- candidate generators
-// pre(c) loads what every candidate of the set shares at chunk c (binary: the right row;
-// unary: the word metadata); word(t, c, pre) gives words 2c, 2c+1 of candidate t.
+// pre(c) loads everything of chunk c that the set's candidates read from global memory
+// (binary: the right row; unary: the source row and the word metadata); word(t, c, pre) gives
+// words 2c, 2c+1 of candidate t from it (and the shared-memory tile).  A sweep that stores
+// words can so issue the loads of several chunks before its first store.
 template <int OPC>
 struct BinGen {
+    using Pre = ulonglong2;
     const ulonglong2 *left;   // shared-memory tile, row stride nch
     const ulonglong2 *right;  // global right row
     int nch;
     int rop;
-    __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldcg(right + c); }
+    __device__ __forceinline__ Pre pre(int c) const { return __ldcg(right + c); }
     __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 r) const {
         if (OPC == OP_U) {
             const ulonglong2 l = left[(t >> 1) * nch + c];
@@ -103,19 +107,23 @@ struct BinGen {
 };
 
 // Candidate t of a fused unary row: operator slot t (0 ~, 1 X, 2 F, 3 G) of one source row.
+struct UnPre {
+    ulonglong2 m, s;  // word metadata, source words
+};
 struct UnGen {
+    using Pre = UnPre;
     const ulonglong2 *src;
     const ulonglong2 *meta;
-    __device__ __forceinline__ ulonglong2 pre(int c) const { return __ldcg(meta + c); }
-    __device__ __forceinline__ ulonglong2 word(int t, int c, ulonglong2 m) const {
-        const ulonglong2 s = __ldcg(src + c);
+    __device__ __forceinline__ Pre pre(int c) const { return UnPre{__ldcg(meta + c), __ldcg(src + c)}; }
+    __device__ __forceinline__ ulonglong2 word(int t, int, const Pre &p) const {
         const int op = unary_slot_op(t);
-        return make_ulonglong2(unary_word(op, s.x, m.x & LENMASK), unary_word(op, s.y, m.y & LENMASK));
+        return make_ulonglong2(unary_word(op, p.s.x, p.m.x & LENMASK), unary_word(op, p.s.y, p.m.y & LENMASK));
     }
 };
 
 // A stored row as its own candidate (letters).
 struct RowGen {
+    using Pre = ulonglong2;
     const ulonglong2 *r;
     __device__ __forceinline__ ulonglong2 pre(int c) const { return r[c]; }
     __device__ __forceinline__ ulonglong2 word(int, int, ulonglong2 p) const { return p; }
@@ -293,14 +301,23 @@ __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost,
             if (lane == leader) base = atomicAdd(&C->row_count, (u64)__popc(cm));
             base = __shfl_sync(FULL, base, leader);
             const u64 cap = (u64)A.cap_rows;
-#pragma unroll 1
-            for (int c = lane; c < nch; c += 32) {
-                const ulonglong2 p = g.pre(c);
+            // WU chunks per lane are loaded before any of their words is stored: the stores go
+            // to the same cache as the loads, so the compiler keeps them in program order
+            for (int c0 = lane; c0 < nch; c0 += 32 * WU) {
+                typename Gen::Pre pv[WU];
 #pragma unroll
-                for (int t = 0; t < NC; ++t) {
-                    if ((cm >> t) & 1u) {
-                        const u64 row = base + __popc(cm & ((1u << t) - 1u));
-                        if (row < cap) reinterpret_cast<ulonglong2 *>(A.cache + row * pitch)[c] = g.word(t, c, p);
+                for (int u = 0; u < WU; ++u)
+                    if (c0 + 32 * u < nch) pv[u] = g.pre(c0 + 32 * u);
+#pragma unroll
+                for (int u = 0; u < WU; ++u) {
+                    const int c = c0 + 32 * u;
+                    if (c >= nch) break;
+#pragma unroll
+                    for (int t = 0; t < NC; ++t) {
+                        if ((cm >> t) & 1u) {
+                            const u64 row = base + __popc(cm & ((1u << t) - 1u));
+                            if (row < cap) reinterpret_cast<ulonglong2 *>(A.cache + row * pitch)[c] = g.word(t, c, pv[u]);
+                        }
                     }
                 }
             }
@@ -356,7 +373,7 @@ __device__ __forceinline__ void resolve(const InstArgs &A, InstCtl *C, int cost,
                     vr[t] = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)__shfl_sync(FULL, myv, t) * pitch);
 #pragma unroll 1
                 for (int c = lane; c < nch; c += 32) {
-                    const ulonglong2 p = g.pre(c);
+                    const auto p = g.pre(c);
 #pragma unroll
                     for (int t = 0; t < NC; ++t) {
                         if ((vm >> t) & 1u) {

@@ -216,3 +216,14 @@ def test_costs_and_splits_beyond_old_caps():
     splits = max(sum(1 for i in nonempty if 2 * i <= c - cop and (c - i - cop) in nonempty)
                  for c in range(601) for cop in (costs[2], costs[3], costs[7]))
     assert splits > 64, splits
+
+
+def test_level_stamps_are_ordered(engine):
+    """record_levels: every level with candidates reports when its plan was published, its first
+    item claimed and its first row begun, in that order and within the level's time."""
+    inst = gen.generate(2, 3, 500, 500, 16, 32, 0.5, 9)
+    res = engine.learn(inst, neg_type=1, max_cost=7, stop_at_found=False, record_levels=True)
+    levels = [lv for lv in res.levels if lv["candidates"] > 0]
+    assert len(levels) >= 5
+    for lv in levels:
+        assert 0 < lv["plan_us"] <= lv["claim_us"] <= lv["start_us"] <= lv["ms"] * 1e3, lv

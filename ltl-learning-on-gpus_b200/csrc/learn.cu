@@ -47,6 +47,7 @@ constexpr int ENTRY_CACHE = 256;               // item starts of a plan's first 
 constexpr int NWARPS = LEVEL_THREADS / 32;
 constexpr int NCONS = NWARPS - 1;              // consumer warps per CTA
 static_assert(NCONS == LEVEL_CONSUMERS, "consumer warps");
+constexpr unsigned long long SPLIT_MAX_CANDS = 8192;  // levels below: rows split over warps (8k, 64k, 512k measured)
 constexpr int WU = 1;  // chunks per lane loaded per round of a claim's write sweep (2 and 4 measured slower)
 
 constexpr u64 PIPE_WAIT_NS = 30000000000ull;   // a consumer's wait for the producer (beyond every producer bound)
@@ -75,6 +76,8 @@ struct Slot {
     int stop;                 // remaining rows are skipped (a find at or before this entry)
     int inst;                 // the item's instance (index into Launch::args)
     int trace_first;          // the producer's first item of this plan (level stamps)
+    int split;                // units per row: 1, or (a small level) one per left row / unary operator
+    int units;                // nrows * split: what the consumers take
     int overflowed;           // the cache had overflowed when the item was claimed (or a claim here
                               // overflowed): the rows' new CSs take no hash slots
     InstArgs args;            // its arguments as they were when the item was claimed (a batch slot's
@@ -460,11 +463,11 @@ __device__ __forceinline__ void finish(const InstArgs &A, InstCtl *C, Slot &sl, 
 // are in flight per lane.  Positives are the first npos words, so acceptance needs no metadata.
 template <int OPC, int TL, int HK>
 __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &sl, const ulonglong2 *tile,
-                                           const ulonglong2 *R, long long r, int lane) {
+                                           int nl, long long l_first, const ulonglong2 *R, long long r, int lane) {
     constexpr int TLP = OPC == OP_U ? TL / 2 : TL;
     constexpr int NC = TL;
     const int nch = A.pitch >> 1, npos = A.npos, n = A.n;
-    const int nl = sl.nl, rop = sl.op;
+    const int rop = sl.op;
     u64 h[NC];
 #pragma unroll
     for (int t = 0; t < NC; ++t) h[t] = 0;
@@ -513,7 +516,6 @@ __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &
     const int cnt = OPC == OP_U ? 2 * nl : nl;
     const u32 valid = cnt >= 32 ? FULL : ((1u << cnt) - 1u);
     const BinGen<OPC> g{tile, R, nch, rop};
-    const long long l_first = sl.l_first;
     finish<NC>(A, C, sl, g, h, bp, bn, valid,
                [&](int t) {
                    if (OPC == OP_U) {
@@ -534,11 +536,10 @@ __device__ __forceinline__ void binary_row(const InstArgs &A, InstCtl *C, Slot &
 
 // Unary row: every operator of the slot's mask on source row s (at src; one load of each chunk).
 template <int HK>
-__device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &sl, const ulonglong2 *src, long long s,
-                                          int lane) {
+__device__ __forceinline__ void unary_row(const InstArgs &A, InstCtl *C, Slot &sl, int mask, const ulonglong2 *src,
+                                          long long s, int lane) {
     constexpr int NC = 4;
     const int nch = A.pitch >> 1, npos = A.npos, n = A.n;
-    const int mask = sl.op;
     const ulonglong2 *meta = reinterpret_cast<const ulonglong2 *>(A.wmeta);
     u64 h[NC] = {0, 0, 0, 0};
     u32 bp = 0, bn = 0;
@@ -1310,6 +1311,7 @@ struct ProdCache {
     int rc, ur, cost, check_only;
     long long plan_items;
     int trace_first;      // the next item filled is this producer's first of the plan
+    int split_small;      // the plan's level has fewer than SPLIT_MAX_CANDS candidates
     long long item0[ENTRY_CACHE];
     Entry e;
     InstArgs a;           // the instance's arguments (read once per plan)
@@ -1473,6 +1475,7 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
                 pc.cost = cost;
                 pc.check_only = chk;
                 pc.plan_items = pitems;
+                pc.split_small = __ldcg(&C->plan.cand) < SPLIT_MAX_CANDS;
                 pc.trace_first = pc.a.level_ns != nullptr;
                 if (pc.trace_first) atomicCAS(pc.a.level_ns + (u64)cost * LEVEL_TRACE + LT_CLAIMED, 0ull, globaltimer());
             }
@@ -1518,6 +1521,13 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
                                         pc.plan_items, skip, pc.a.pitch);
             sl.trace_first = pc.trace_first;
             sl.overflowed = ovf ? 1 : 0;
+            // a small level's rows are split into one unit per left row / unary operator, so
+            // more warps share its few rows (one warp's pass over a whole row is what such a
+            // level costs)
+            int split = 1;
+            if (!skip && pc.split_small) split = sl.kind == ENT_UNARY ? __popc((unsigned)sl.op) : sl.nl;
+            sl.split = max(1, split);
+            sl.units = sl.nrows * sl.split;
             pc.trace_first = 0;
             if (!skip) {
                 const u64 pitch = (u64)pc.a.pitch;
@@ -1560,24 +1570,34 @@ __device__ __forceinline__ int take_rows(Slot &sl, int kind, const ulonglong2 *t
         unsigned idx = 0;
         if (lane == 0) idx = atomicAdd(&sl.next_row, 1u);
         idx = __shfl_sync(FULL, idx, 0);
-        if ((int)idx >= sl.nrows) break;
+        if ((int)idx >= sl.units) break;
         if (idx == 0 && sl.trace_first && lane == 0)
             atomicCAS(A.level_ns + (u64)sl.cost * LEVEL_TRACE + LT_STARTED, 0ull, globaltimer());
         if (!*(volatile int *)&sl.stop) {
-            const long long r = sl.row0 + idx;
+            // a unit is a row, or with split one left row (binary) or one operator (unary) of it
+            const int split = sl.split, part = (int)idx % split;
+            const long long r = sl.row0 + (int)idx / split;
             const ulonglong2 *rp = reinterpret_cast<const ulonglong2 *>(A.cache + (u64)r * A.pitch);
-            if (kind == ENT_UNARY)
-                unary_row<HK>(A, C, sl, rp, r, lane);
-            else if (kind == ENT_ANDOR)
-                binary_row<OP_ANDOR_CLASS, TL, HK>(A, C, sl, tile, rp, r, lane);
-            else
-                binary_row<OP_U, TL, HK>(A, C, sl, tile, rp, r, lane);
+            if (kind == ENT_UNARY) {
+                int mask = sl.op;
+                for (int q = 0; q < part && split > 1; ++q) mask &= mask - 1;  // the part-th operator
+                unary_row<HK>(A, C, sl, split > 1 ? (mask & -mask) : mask, rp, r, lane);
+            } else {
+                const int nch = A.pitch >> 1;
+                const ulonglong2 *t0 = split > 1 ? tile + (u64)part * (u64)nch : tile;
+                const int nl = split > 1 ? 1 : sl.nl;
+                const long long lf = sl.l_first + (split > 1 ? part : 0);
+                if (kind == ENT_ANDOR)
+                    binary_row<OP_ANDOR_CLASS, TL, HK>(A, C, sl, t0, nl, lf, rp, r, lane);
+                else
+                    binary_row<OP_U, TL, HK>(A, C, sl, t0, nl, lf, rp, r, lane);
+            }
         }
         unsigned d = 0;
         __threadfence_block();  // this row's evals count is in before the row counts as done
         if (lane == 0) d = atomicAdd(&sl.rows_done, 1u);
         d = __shfl_sync(FULL, d, 0);
-        if ((int)d + 1 == sl.nrows) {  // the item is done
+        if ((int)d + 1 == sl.units) {  // the item is done
             u64 dd = 0;
             if (lane == 0) {
                 const unsigned ev = atomicAdd(&sl.evals, 0u);

@@ -1557,9 +1557,11 @@ __device__ void producer(const Launch &L, unsigned char *smem, u64 *tiles, int l
     __syncwarp();
 }
 
-// The rows of one slot a consumer warp takes, until the slot has none left.  Returns
-// SLOT_CLOSE when this warp finished the level's last item, else SLOT_NEXT; closing the level
-// (with the slot's arguments, before the slot is released) is the caller's.
+// The units of one slot a consumer warp takes, until the slot has none left: a unit is one row
+// of the item, or at a small level (split > 1) one left row of the tile against one right row,
+// or one unary operator on one source row.  Returns SLOT_CLOSE when this warp finished the
+// level's last item, else SLOT_NEXT; closing the level (with the slot's arguments, before the
+// slot is released) is the caller's.
 enum { SLOT_NEXT = 0, SLOT_CLOSE = 1 };
 template <int TL, int HK>
 __device__ __forceinline__ int take_rows(Slot &sl, int kind, const ulonglong2 *tile, int lane) {
